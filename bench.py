@@ -1,0 +1,328 @@
+"""Benchmark of the B200 point-set hot path: Gaussian kernel pair-evaluations per second.
+
+Workload ("L6 kernel sums", the deformation-kernel sums of the level-6 registration): source vertices of the
+level-6 icosphere (N = M = 40,962), smoothed momenta a = K_0.3 (N(0, 0.1^2)), Gaussian widths sigma = 0.25
+and 0.5. One step = K(x, x) a for both widths (2 * N^2 pair evaluations), FP32 pair arithmetic with
+compensated accumulation and FP64 outputs.
+
+  value     pairs/s with inputs resident in HBM, device-timed (CUDA events per step, L2 flushed between steps
+            by writing a 256 MiB buffer; the flush is outside the timed events)
+  e2e       the same step through the reference-facing API `Kernel.applyK(x, a)` with numpy (host) arrays:
+            host->device copy of x and a, the kernels, device->host copy of the result, every step
+  roofline  the pair kernel against the FP32 pipe: 9 FP32 lane-ops + 1 SFU op per pair;
+            peak = 148 SMs x 128 FP32 lanes x max SM clock
+  cpu_baseline  the CPU oracle (numba, float64, all host threads) on a bounded sample of the same sums
+
+`--impl reference` times the CPU implementation of the same sums (the oracle restatement of the reference's
+numba kernels, all host threads) and prints the same metric with "impl": "reference".
+
+Multi-GPU (torchrun): every rank runs the same workload on its own GPU (independent replicas, weak scaling);
+times are the max over ranks; value = pairs of all ranks / that time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, 'py-lddmm_b200'))
+sys.path.insert(0, REPO)
+
+LEVEL = 6
+SIGMAS = (0.25, 0.5)
+OPS_FP32_PER_PAIR = 9
+OPS_SFU_PER_PAIR = 1
+METRIC = 'Gauss kernel pairs/s'
+
+
+def workload():
+    from base.syntheticShapes import icosphere
+    x, _ = icosphere(LEVEL)
+    rng = np.random.default_rng(1)
+    a_raw = rng.normal(0.0, 0.1, size=x.shape)
+    return x, a_raw
+
+
+def config(n):
+    return {'workload': 'L6 kernel sums: K(x,x)a, icosphere level 6, N=M=%d, sigma in %s, smoothed momenta' % (
+        n, list(SIGMAS)), 'level': LEVEL, 'n_points': n, 'sigmas': list(SIGMAS), 'op': 'applyK (Gaussian)',
+        'l2': 'flushed between timed steps (256 MiB write)'}
+
+
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(REPO, 'gpurun_out', f'clocks_gpu{gpu_index}.csv')
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+        try:
+            self.fh = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), f'--query-gpu={q}', '--format=csv,noheader,nounits',
+                                          '-lms', '100'], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        try:
+            for line in open(self.path):
+                f = [t.strip() for t in line.split(',')]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == 'active':
+                        reasons.add(nm)
+        except OSError:
+            pass
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(mx), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, 'MEASURED_PEAKS.json')
+    try:
+        return json.load(open(p))
+    except Exception:
+        return {}
+
+
+def ncu_traffic():
+    """dram bytes per launch of the pair kernel from the committed ncu summary (profiles/)."""
+    p = os.path.join(REPO, 'profiles', 'applyk_pairs_L6_ncu.json')
+    try:
+        d = json.load(open(p))
+        return d.get('dram_bytes_per_launch')
+    except Exception:
+        return None
+
+
+def cpu_baseline(x, a, n_targets, threads):
+    """Oracle (numba float64) on a bounded sample: n_targets targets x all sources, both widths."""
+    import oracle as O
+    y = x[:n_targets]
+    O.apply_k(y[:64], x[:64], a[:64], SIGMAS[0])      # JIT warm-up
+    t0 = time.perf_counter()
+    for s in SIGMAS:
+        O.apply_k(y, x, a, s)
+    dt = time.perf_counter() - t0
+    pairs = len(SIGMAS) * y.shape[0] * x.shape[0]
+    return pairs / dt, dt, pairs
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import numba
+    threads = os.cpu_count() or 1
+    numba.set_num_threads(threads)
+    x, a_raw = workload()
+    import oracle as O
+    t0 = time.perf_counter()
+    a = O.apply_k(x, x, a_raw, 0.3)        # momentum smoothing (setup, untimed)
+    setup = time.perf_counter() - t0
+    n_t = args.ref_targets
+    for _ in range(args.warmup):
+        O.apply_k(x[:256], x, a, SIGMAS[0])
+    vals = []
+    for _ in range(args.steps):
+        v, dt, pairs = cpu_baseline(x, a, n_t, threads)
+        vals.append((v, dt, pairs))
+    tot_pairs = sum(p for _, _, p in vals)
+    tot_t = sum(d for _, d, _ in vals)
+    value = tot_pairs / tot_t
+    line = {'metric': METRIC, 'value': value, 'unit': 'pairs/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * tot_t / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
+            'config': config(x.shape[0]),
+            'cpu_baseline': {'value': value, 'unit': 'pairs/s', 'cores': threads, 'kind': 'port',
+                             'sample': f'{n_t} targets x {x.shape[0]} sources x {len(SIGMAS)} widths per step '
+                                       f'(oracle numba restatement of ku.applyK_numba, float64)'},
+            'e2e': {'value': value, 'unit': 'pairs/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+            'setup_s': setup}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from base import _native as nat
+    from base.kernelFunctions import Kernel
+
+    torch.cuda.set_device(local_rank)
+    x, a_raw = workload()
+    n = x.shape[0]
+    X = torch.from_numpy(x).cuda()
+    K03 = Kernel(name='gauss', sigma=0.3)
+    K03.pk_dtype = 'float32'
+    A = K03.applyK(X, torch.from_numpy(a_raw).cuda())
+    a = A.cpu().numpy()
+    lib = nat.lib()
+    origin = nat.centroid(X)
+    o = nat.origin_arg(origin)
+    outs = [torch.empty((n, 3), dtype=torch.float64, device='cuda') for _ in SIGMAS]
+    ws, wsb = nat.workspace(n, n, nat.FP32C)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+    stream = torch.cuda.current_stream()
+    sp = nat.stream_ptr()
+
+    def step(evs=None):
+        for i, s in enumerate(SIGMAS):
+            if evs is not None:
+                evs[i][0].record(stream)
+            rc = lib.lddmm_apply_k(nat.ptr(X), n, nat.ptr(X), nat.ptr(A), n, s, o, nat.ptr(outs[i]), nat.FP32C, ws,
+                                   wsb, sp)
+            if evs is not None:
+                evs[i][1].record(stream)
+            if rc != 0:
+                raise RuntimeError(f'lddmm_apply_k failed: {rc}')
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = 0
+    step_ms, launch_ms = [], []
+    with ClockSampler(local_rank if 'CUDA_VISIBLE_DEVICES' not in os.environ else local_rank) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in SIGMAS]
+            step(evs)
+            launches += 2 * len(SIGMAS)
+            torch.cuda.synchronize()
+            ms = [e0.elapsed_time(e1) for e0, e1 in evs]
+            launch_ms += ms
+            step_ms.append(sum(ms))
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device='cuda')
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t)
+    pairs_per_step = len(SIGMAS) * n * n
+    value = world * pairs_per_step * args.steps / (total_ms * 1e-3)
+
+    # end-to-end through the reference-facing API (numpy in / numpy out)
+    K = {s: Kernel(name='gauss', sigma=s) for s in SIGMAS}
+    for k in K.values():
+        k.pk_dtype = 'float32'
+    for _ in range(max(1, args.warmup)):
+        for s in SIGMAS:
+            K[s].applyK(x, a)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in SIGMAS:
+            r = K[s].applyK(x, a)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        launches += 2 * len(SIGMAS)
+    te = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device='cuda')
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * pairs_per_step * args.steps / (float(te) * 1e-3)
+    h2d = len(SIGMAS) * (x.nbytes + a.nbytes)
+    d2h = len(SIGMAS) * r.nbytes
+
+    if rank != 0:
+        return
+    clocks = clk.summary()
+    peaks = measured_peaks()
+    sm_max = clocks.get('sm_max_mhz') or peaks.get('sm_max_mhz') or 1965.0
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    peak_fp32 = n_sm * 128 * sm_max * 1e6 / 1e12          # T lane-ops/s
+    mean_launch_s = statistics.mean(launch_ms) * 1e-3
+    achieved = n * n * OPS_FP32_PER_PAIR / mean_launch_s / 1e12
+    sfu_frac = (n * n * OPS_SFU_PER_PAIR / mean_launch_s) / (n_sm * 16 * sm_max * 1e6)
+    traffic = ncu_traffic()
+    cb_targets = args.cpu_targets
+    import numba
+    numba.set_num_threads(os.cpu_count() or 1)
+    cb_val, cb_dt, cb_pairs = cpu_baseline(x, a, cb_targets, os.cpu_count())
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'pairs/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f32 (compensated) -> f64', 'data': 'synthetic', 'config': config(n),
+        'e2e': {'value': e2e_value, 'unit': 'pairs/s', 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
+                'ms_per_step': float(te) / args.steps, 'api': 'Kernel.applyK(numpy x, numpy a)'},
+        'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak_fp32, 'unit': 'T FP32 lane-ops/s',
+                     'frac': achieved / peak_fp32, 'sfu_frac': sfu_frac, 'traffic': traffic,
+                     'kernel': 'pairs_kernel<OpK<float>> (+ epilogue, timed together per call)',
+                     'ops_per_pair': {'fp32': OPS_FP32_PER_PAIR, 'sfu': OPS_SFU_PER_PAIR},
+                     'peak_source': f'{n_sm} SMs x 128 FP32 lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
+                                    f'max SM clock; MEASURED_PEAKS.json has no FP32 figure)'},
+        'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': os.cpu_count(), 'kind': 'port',
+                         'sample': f'{cb_targets} targets x {n} sources x {len(SIGMAS)} widths, float64 numba oracle, '
+                                   f'{cb_dt:.2f} s'},
+        'clocks': clocks, 'gpu_launches': launches,
+        'pairs_per_step': pairs_per_step,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--cpu-targets', type=int, default=4096)
+    ap.add_argument('--ref-targets', type=int, default=2048)
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

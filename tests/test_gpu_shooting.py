@@ -1,0 +1,111 @@
+"""Parity of the fused shooting / adjoint kernels with the reference (base/pointEvolution.py).
+
+Tolerance (relative L2 error against float64): FP32 compensated path 2e-5, FP64 path 1e-11.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = {'float32': 2e-5, 'float64': 1e-11}
+
+
+def kernel(sigma, dtype):
+    from base.kernelFunctions import Kernel
+    K = Kernel(name='gauss', sigma=sigma)
+    K.pk_dtype = dtype
+    return K
+
+
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+def test_first_order_vs_reference(dtype):
+    from base import pointEvolution as evol
+    d = np.load(os.path.join(GOLDEN, 'first_order_L2.npz'))
+    K = kernel(float(d['sigma']), dtype)
+    st = evol.landmarkDirectEvolutionEuler(d['x0'], d['at'], K)
+    assert rel_err(st['xt'], d['xt']) < TOL[dtype]
+    dat, xt, pxt = evol.landmarkHamiltonianGradient(d['x0'], d['at'], d['px1'], K, float(d['regweight']),
+                                                    getCovector=True)
+    assert rel_err(dat, d['dat']) < TOL[dtype]
+    assert rel_err(pxt, d['pxt']) < TOL[dtype]
+
+
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+def test_second_order_vs_reference(dtype):
+    from base import pointEvolution as evol
+    d = np.load(os.path.join(GOLDEN, 'second_order_L2.npz'))
+    K = kernel(float(d['sigma']), dtype)
+    g = evol.secondOrderGradient(d['x0'], d['a0'], d['px1'], d['pa1'], K, float(d['timeStep']))
+    for k in ('xt', 'at', 'da0', 'pxt', 'pat'):
+        assert rel_err(g[k], d[k]) < TOL[dtype], (k, rel_err(g[k], d[k]))
+    fw = evol.secondOrderEvolution(d['x0'], d['a0'], K, float(d['timeStep']))
+    assert rel_err(fw['xt'], d['xt']) < TOL[dtype]
+
+
+def test_second_order_l4_vs_oracle():
+    import oracle as O
+    from base import pointEvolution as evol
+    from base.syntheticShapes import icosphere
+    x0, _ = icosphere(4)
+    rng = np.random.default_rng(5)
+    a0 = O.apply_k(x0, x0, rng.normal(0, 0.3, x0.shape), 0.4)
+    px1 = rng.normal(0, 0.5, x0.shape)
+    pa1 = np.zeros_like(x0)
+    ref = O.second_order_gradient(x0, a0, px1, pa1, 0.5, 0.1)
+    g = evol.secondOrderGradient(x0, a0, px1, pa1, kernel(0.5, 'float32'), 0.1)
+    for k in ('xt', 'at', 'da0', 'pxt', 'pat'):
+        assert rel_err(g[k], ref[k]) < 2e-5, (k, rel_err(g[k], ref[k]))
+
+
+def test_step_entry_points_match_trajectory():
+    """The per-step C-ABI calls reproduce the whole-trajectory calls exactly (same kernels, same order)."""
+    import torch
+    from base import _native as nat
+    from base import pointEvolution as evol
+    from base.syntheticShapes import icosphere
+    x0, _ = icosphere(3)
+    rng = np.random.default_rng(6)
+    X0 = torch.from_numpy(x0).cuda()
+    A0 = torch.from_numpy(rng.normal(0, 0.2, x0.shape)).cuda()
+    K = kernel(0.5, 'float32')
+    o = nat.centroid(X0)
+    xt, at = evol.shoot_second_order(X0, A0, K, 0.1, origin=o)
+    x, a = X0.clone(), A0.clone()
+    ws, wsb = nat.workspace(x0.shape[0], x0.shape[0])
+    for t in range(10):
+        x1, a1 = torch.empty_like(x), torch.empty_like(a)
+        nat.check(nat.lib().lddmm_second_order_step(nat.ptr(x), nat.ptr(a), x.shape[0], 0.5, 0.1, nat.origin_arg(o),
+                                                    nat.ptr(x1), nat.ptr(a1), 0, ws, wsb, nat.stream_ptr()))
+        x, a = x1, a1
+    assert torch.equal(x, xt[-1]) and torch.equal(a, at[-1])
+    px = torch.from_numpy(rng.normal(size=x0.shape)).cuda()
+    pa = torch.zeros_like(px)
+    pxt, pat, _ = evol.second_order_adjoint(xt, at, px, pa, K, 0.1, origin=o)
+    for t in range(9, -1, -1):
+        p0, q0 = torch.empty_like(px), torch.empty_like(pa)
+        nat.check(nat.lib().lddmm_second_order_adjoint_step(nat.ptr(xt[t]), nat.ptr(at[t]), nat.ptr(px), nat.ptr(pa),
+                                                            x.shape[0], 0.5, 0.1, nat.origin_arg(o), nat.ptr(p0),
+                                                            nat.ptr(q0), 0, ws, wsb, nat.stream_ptr()))
+        px, pa = p0, q0
+    assert torch.equal(px, pxt[0]) and torch.equal(pa, pat[0])
+
+
+def test_first_order_energy_and_euclidean_gradient():
+    import torch
+    import oracle as O
+    from base import pointEvolution as evol
+    d = np.load(os.path.join(GOLDEN, 'first_order_L2.npz'))
+    K = kernel(0.5, 'float64')
+    X0, AT = torch.from_numpy(d['x0']).cuda(), torch.from_numpy(d['at']).cuda()
+    e = torch.zeros(1, dtype=torch.float64, device='cuda')
+    xt = evol.shoot_first_order(X0, AT, K, regweight=0.8, energy=e)
+    T = AT.shape[0]
+    ref = sum(0.8 / T * (d['at'][t] * O.apply_k(d['xt'][t], d['xt'][t], d['at'][t], 0.5)).sum() for t in range(T))
+    assert abs(float(e) - ref) < 1e-12 * abs(ref)
+    pxt, dat = evol.first_order_gradient(xt, AT, torch.from_numpy(d['px1']).cuda(), K, 0.8, euclidean=True)
+    for t in range(T):
+        g = 2 * 0.8 * d['at'][t] - d['pxt'][t + 1]
+        assert rel_err(dat[t].cpu().numpy(), O.apply_k(d['xt'][t], d['xt'][t], g, 0.5)) < 1e-11

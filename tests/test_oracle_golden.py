@@ -1,0 +1,99 @@
+"""The CPU oracle against golden fixtures produced by running the reference itself (tests/golden/make_golden.py).
+
+This pins the oracle: every CUDA parity test compares against the oracle, and the oracle is pinned here to the
+reference's own float64 outputs (numba / numpy paths of base/kernelFunctions_util.py, base/pointEvolution.py,
+base/surfaceDistances.py).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN, rel_err
+
+TOL = 1e-12
+
+KFILES = sorted(glob.glob(os.path.join(GOLDEN, 'kernels_*.npz')))
+DFILES = sorted(glob.glob(os.path.join(GOLDEN, 'data_*.npz')))
+
+
+def test_fixtures_present():
+    assert len(KFILES) == 4 and len(DFILES) == 4
+    for name in ('first_order_L2', 'second_order_L2', 'matching_first_L2', 'matching_second_L2'):
+        assert os.path.exists(os.path.join(GOLDEN, name + '.npz'))
+
+
+@pytest.mark.parametrize('path', KFILES, ids=os.path.basename)
+def test_kernel_operators(path):
+    d = np.load(path)
+    s = float(d['sigma'])
+    x, y, a, p, q = d['x'], d['y'], d['a'], d['p'], d['q']
+    ny = y.shape[0]
+    assert rel_err(O.apply_k(x, x, a, s), d['applyK']) < TOL
+    assert rel_err(O.apply_k(y, x, a, s), d['applyK_cross']) < TOL
+    assert rel_err(O.apply_diff_kt(x, x, p, a, s), d['applyDiffKT']) < TOL
+    assert rel_err(O.apply_diff_kt(y, x, p[:ny], a, s), d['applyDiffKT_cross']) < TOL
+    assert rel_err(O.apply_diff_kt(x, x, p, a, s, sym=True), d['applyDiffKT_sym']) < TOL
+    assert rel_err(O.apply_diff_kt(x, x, p, a, s, lddmm=True, regweight=float(d['regweight'])),
+                   d['applyDiffKT_lddmm']) < TOL
+    assert rel_err(O.apply_ddiff_k11and12(x, a, q, p, s), d['applyDDiffK11and12']) < TOL
+    assert rel_err(O.apply_diff_k1and2(x, p, a, s), d['applyDiffK1and2']) < TOL
+    assert rel_err(O.apply_divergence(x, x, a, s), d['applyDivergence']) < TOL
+    assert rel_err(O.apply_divergence(y, x, a, s), d['applyDivergence_cross']) < TOL
+    w, b = d['ay'], d['betay']
+    assert rel_err(O.apply_k_tensor(x, x, w, w, b, b, s), d['applyKTensor']) < TOL
+    assert rel_err(O.apply_k_tensor(y, x, w[:ny], w, b[:ny], b, s), d['applyKTensor_cross']) < TOL
+    if 'beta' in d:
+        assert rel_err(O.apply_diff_k_mat(x, x, d['beta'], s), d['applyDiffKmat']) < TOL
+        assert rel_err(O.apply_k_mat(x, x, d['u'], s), d['applyK_mat']) < TOL
+
+
+def test_first_order_shooting():
+    d = np.load(os.path.join(GOLDEN, 'first_order_L2.npz'))
+    s, w = float(d['sigma']), float(d['regweight'])
+    assert rel_err(O.landmark_direct_evolution_euler(d['x0'], d['at'], s), d['xt']) < TOL
+    dat, xt, pxt = O.landmark_hamiltonian_gradient(d['x0'], d['at'], d['px1'], s, w)
+    assert rel_err(dat, d['dat']) < TOL
+    assert rel_err(pxt, d['pxt']) < TOL
+
+
+def test_second_order_shooting():
+    d = np.load(os.path.join(GOLDEN, 'second_order_L2.npz'))
+    g = O.second_order_gradient(d['x0'], d['a0'], d['px1'], d['pa1'], float(d['sigma']), float(d['timeStep']))
+    for k in ('xt', 'at', 'da0', 'pxt', 'pat'):
+        assert rel_err(g[k], d[k]) < 1e-12, k
+
+
+@pytest.mark.parametrize('path', DFILES, ids=os.path.basename)
+def test_surface_terms(path):
+    d = np.load(path)
+    s, F, x1, xd, w = float(d['sigma']), d['faces'], d['x1'], d['xdef'], d['weights']
+    assert rel_err(O.varifold_norm0(x1, F, s), d['varifoldNorm0']) < TOL
+    assert rel_err(O.varifold_norm_def(xd, F, x1, F, s), d['varifoldNormDef']) < TOL
+    assert rel_err(O.varifold_norm_gradient(xd, F, x1, F, s), d['varifoldNormGradient']) < 1e-12
+    assert rel_err(O.varifold_norm_def(xd, F, x1, F, s, weights=w), d['varifoldNormDef_w']) < TOL
+    assert rel_err(O.varifold_norm_gradient(xd, F, x1, F, s, weights=w), d['varifoldNormGradient_w']) < 1e-12
+    assert rel_err(O.current_norm0(x1, F, s), d['currentNorm0']) < TOL
+    assert rel_err(O.current_norm_def(xd, F, x1, F, s), d['currentNormDef']) < TOL
+    assert rel_err(O.current_norm_gradient(xd, F, x1, F, s), d['currentNormGradient']) < 1e-12
+    assert rel_err(O.measure_norm0(x1, F, s), d['measureNorm0']) < TOL
+    assert rel_err(O.measure_norm_def(xd, F, x1, F, s), d['measureNormDef']) < TOL
+    assert rel_err(O.measure_norm_gradient(xd, F, x1, F, s), d['measureNormGradient']) < 1e-12
+
+
+def test_varifold_weight_gradient_fd():
+    """with_weights=True cannot be pinned on the reference under numpy 2 (it raises). The reference's weight
+    gradient carries an extra face-weight factor (z1w = 2/3 fw a (...), base/surfaceDistances.py:555-563), so it is
+    the exact derivative with respect to the vertex weights at unit weights: checked there by central FD."""
+    d = np.load(os.path.join(GOLDEN, 'data_L2_s0.3.npz'))
+    s, F, x1, xd = float(d['sigma']), d['faces'], d['x1'], d['xdef']
+    w = np.ones(xd.shape[0])
+    _, pxw = O.varifold_norm_gradient(xd, F, x1, F, s, weights=w, with_weights=True)
+    rng = np.random.default_rng(3)
+    dw = rng.normal(size=w.shape)
+    h = 1e-6
+    fd = (O.varifold_norm_def(xd, F, x1, F, s, weights=w + h * dw)
+          - O.varifold_norm_def(xd, F, x1, F, s, weights=w - h * dw)) / (2 * h)
+    assert abs(fd - (pxw * dw).sum()) < 1e-6 * max(1.0, abs(fd))
