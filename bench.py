@@ -55,23 +55,48 @@ def config(n):
 
 
 class ClockSampler:
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
+    """nvidia-smi sampling (50 ms) of SM clock and throttle reasons; samples are kept for the timed window only
+    (window = [mark_start, mark_end] wall clock, widened to the nearest samples when shorter than the period)."""
+
+    NAMES = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+
+    def __init__(self, device_index):
+        self.dev = device_index
         self.proc = None
-        self.path = os.path.join(REPO, 'gpurun_out', f'clocks_gpu{gpu_index}.csv')
+        self.t0 = self.t1 = None
+        self.path = os.path.join(REPO, 'gpurun_out', f'clocks_rank{device_index}.csv')
+
+    def _gpu_id(self):
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return u if u.startswith('GPU-') else 'GPU-' + u
+        except Exception:
+            return str(self.dev)
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
-        q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+        q = ('timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
         try:
             self.fh = open(self.path, 'w')
-            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), f'--query-gpu={q}', '--format=csv,noheader,nounits',
-                                          '-lms', '100'], stdout=self.fh, stderr=subprocess.DEVNULL)
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', self._gpu_id(), f'--query-gpu={q}',
+                                          '--format=csv,noheader,nounits', '-lms', '50'], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+            deadline = time.time() + 5.0
+            while time.time() < deadline and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(0.12)
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -83,27 +108,30 @@ class ClockSampler:
             self.fh.close()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        import datetime
+        rows = []
         try:
             for line in open(self.path):
                 f = [t.strip() for t in line.split(',')]
                 if len(f) < 9:
                     continue
                 try:
-                    sm.append(float(f[1]))
-                    mx.append(float(f[2]))
+                    ts = datetime.datetime.strptime(f[0], '%Y/%m/%d %H:%M:%S.%f').timestamp()
+                    rows.append((ts, float(f[1]), float(f[2]), [v.lower() == 'active' for v in f[5:9]]))
                 except ValueError:
                     continue
-                for nm, v in zip(names, f[5:9]):
-                    if v.lower() == 'active':
-                        reasons.add(nm)
         except OSError:
             pass
-        if not sm:
+        if not rows:
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
-        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(mx), 'reasons': sorted(reasons),
-                'samples': len(sm)}
+        t0 = self.t0 if self.t0 is not None else rows[0][0]
+        t1 = self.t1 if self.t1 is not None else rows[-1][0]
+        sel = [r for r in rows if t0 - 0.06 <= r[0] <= t1 + 0.06]
+        if not sel:   # window shorter than the sampling period: nearest sample after the start
+            sel = [min(rows, key=lambda r: abs(r[0] - t0))]
+        reasons = sorted({nm for r in sel for nm, on in zip(self.NAMES, r[3]) if on})
+        return {'sm_mhz': statistics.median(r[1] for r in sel), 'sm_max_mhz': max(r[2] for r in sel),
+                'reasons': reasons, 'samples': len(sel), 'window_s': round(t1 - t0, 4)}
 
 
 def measured_peaks():
@@ -211,8 +239,9 @@ def run_b200(args, rank, world, local_rank):
         dist.barrier()
     launches = 0
     step_ms, launch_ms = [], []
-    with ClockSampler(local_rank if 'CUDA_VISIBLE_DEVICES' not in os.environ else local_rank) as clk:
+    with ClockSampler(local_rank) as clk:
         torch.cuda.synchronize()
+        clk.mark_start()
         for _ in range(args.steps):
             flush.fill_(1.0)
             evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in SIGMAS]
@@ -223,6 +252,7 @@ def run_b200(args, rank, world, local_rank):
             launch_ms += ms
             step_ms.append(sum(ms))
         torch.cuda.synchronize()
+        clk.mark_end()
     if world > 1:
         dist.barrier()
     total_ms = sum(step_ms)
@@ -298,7 +328,7 @@ def run_b200(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-targets', type=int, default=4096)

@@ -100,3 +100,14 @@ def registration_pair(level, n_bumps=8, amplitude=0.05, width=0.3, seed=0):
     x0, faces = icosphere(level)
     x1 = bumpy_ellipsoid(x0, n_bumps=n_bumps, amplitude=amplitude, width=width, seed=seed)
     return x0, faces, x1
+
+
+def smooth_momenta(x, rng, apply_k, sigma_smooth=0.4, sigma_def=0.5, vmax=0.3):
+    """Random smooth momenta with a prescribed initial speed: a = K_{sigma_smooth} N(0, 1), rescaled so that the
+    velocity K_{sigma_def} a has max norm `vmax`. `apply_k(y, x, a, sigma)` is any Gaussian kernel sum.
+
+    Unnormalised recipes (a = K_s N(0, c^2)) give speeds that grow with the vertex count (7 at 162 vertices, ~400 at
+    2,562 for c = 0.1, s = 0.3) and therefore exploding trajectories; the rescaling keeps every level comparable."""
+    a = apply_k(x, x, rng.normal(size=x.shape), sigma_smooth)
+    v = apply_k(x, x, a, sigma_def)
+    return a * (vmax / np.linalg.norm(v, axis=1).max())

@@ -70,9 +70,10 @@ def load_shapes():
     return m
 
 
-def smooth_momenta(kf, x, rng, scale, sigma):
-    a = rng.normal(0.0, scale, size=x.shape)
-    return kf.Kernel(name='gauss', sigma=sigma).applyK(x, a)
+def smooth_momenta(kf, shapes, x, rng, sigma_smooth, sigma_def=0.5, vmax=0.3):
+    """The package's normalised recipe (syntheticShapes.smooth_momenta) evaluated with the reference's Kernel."""
+    return shapes.smooth_momenta(x, rng, lambda y_, x_, a_, s: kf.Kernel(name='gauss', sigma=s).applyK(x_, a_, firstVar=y_),
+                                 sigma_smooth=sigma_smooth, sigma_def=sigma_def, vmax=vmax)
 
 
 def kernel_fixtures(kf, shapes, out):
@@ -122,13 +123,13 @@ def shooting_fixtures(kf, evol, shapes, out):
     x0, _ = shapes.icosphere(2)
     K = kf.Kernel(name='gauss', sigma=0.5)
     T = 10
-    at = np.stack([smooth_momenta(kf, x0, rng, 0.1, 0.3) for _ in range(T)])
+    at = np.stack([smooth_momenta(kf, shapes, x0, rng, 0.3, vmax=0.3) for _ in range(T)])
     px1 = rng.normal(0.0, 0.5, size=x0.shape)
     st = evol.landmarkDirectEvolutionEuler(x0, at, K)
     dat, xt, pxt = evol.landmarkHamiltonianGradient(x0, at, px1, K, 0.8, getCovector=True)
     out['first_order_L2'] = dict(x0=x0, at=at, px1=px1, sigma=0.5, regweight=0.8,
                                  xt=st['xt'], dat=dat, xt_grad=xt, pxt=pxt)
-    a0 = smooth_momenta(kf, x0, rng, 0.3, 0.4)
+    a0 = smooth_momenta(kf, shapes, x0, rng, 0.4, vmax=0.3)
     fw = evol.secondOrderEvolution(x0, a0, K, 0.1)
     pa1 = rng.normal(0.0, 0.2, size=x0.shape)
     g = evol.secondOrderGradient(x0, a0, px1, pa1, K, 0.1)

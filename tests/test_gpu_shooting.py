@@ -48,10 +48,10 @@ def test_second_order_vs_reference(dtype):
 def test_second_order_l4_vs_oracle():
     import oracle as O
     from base import pointEvolution as evol
-    from base.syntheticShapes import icosphere
+    from base.syntheticShapes import icosphere, smooth_momenta
     x0, _ = icosphere(4)
     rng = np.random.default_rng(5)
-    a0 = O.apply_k(x0, x0, rng.normal(0, 0.3, x0.shape), 0.4)
+    a0 = smooth_momenta(x0, rng, O.apply_k, sigma_smooth=0.4, sigma_def=0.5, vmax=0.3)
     px1 = rng.normal(0, 0.5, x0.shape)
     pa1 = np.zeros_like(x0)
     ref = O.second_order_gradient(x0, a0, px1, pa1, 0.5, 0.1)
