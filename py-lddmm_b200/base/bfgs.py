@@ -1,0 +1,185 @@
+"""Limited-memory BFGS driver of the optimiser protocol (reference: base/bfgs.py:55-313).
+
+The optimisable object `opt` provides getVariable, objectiveFun, updateTry, acceptVarTry, getGradient and
+optionally dotProduct(_euclidean), addProd, prod, copyDir, startOfIteration, endOfIteration, endOfProcedure,
+gradEps, gradCoeff, epsMax, burnIn -- the same protocol as the reference. The two-loop recursion, the initial
+step 1/|q| at the first iteration, the stopping rules (|obj - obj_old| < 1e-7 after burn-in, |grad| < gradEps)
+and the reset-on-failed-line-search logic follow the reference; directions live wherever `opt` keeps them
+(device tensors for the B200 matching classes).
+"""
+import logging
+import time
+from copy import deepcopy
+
+import numpy as np
+
+from .linesearch import line_search_wolfe, line_search_weak_wolfe, line_search_goldstein_price
+
+
+def _dot(x, ys):
+    return [float((x * y).sum()) for y in ys]
+
+
+def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=25, Wolfe=True,
+         lineSearch='Weak_Wolfe'):
+    for need in ('getVariable', 'objectiveFun', 'updateTry', 'acceptVarTry', 'getGradient'):
+        if not hasattr(opt, need):
+            logging.error('Error: required functions are not provided')
+            return
+    line_search = {'Wolfe': line_search_wolfe, 'Goldstein_Price': line_search_goldstein_price,
+                   'Weak_Wolfe': line_search_weak_wolfe}.get(lineSearch, line_search_weak_wolfe)
+    dot = getattr(opt, 'dotProduct_euclidean', None) or getattr(opt, 'dotProduct', None) or _dot
+    addProd = getattr(opt, 'addProd', lambda x, y, a: x + a * y)
+    prod = getattr(opt, 'prod', lambda x, a: a * x)
+    copyDir = getattr(opt, 'copyDir', deepcopy)
+    stopCondition = getattr(opt, 'stopCondition', lambda: True)
+    if hasattr(opt, 'startOptim'):
+        opt.startOptim()
+    if hasattr(opt, 'gradEps'):
+        gradEps = opt.gradEps
+    elif hasattr(opt, 'options') and 'gradEps' in opt.options:
+        gradEps = opt.options['gradEps']
+    else:
+        gradEps = None
+    gradCoeff = getattr(opt, 'gradCoeff', 1.0)
+    epsMax = getattr(opt, 'epsMax', 1.)
+    burnIn = getattr(opt, 'burnIn', 0)
+    eps = epsInit
+    opt.converged = False
+    if getattr(opt, 'reset', False):
+        opt.obj = None
+    obj = opt.objectiveFun()
+    opt.reset = False
+    logging.info('iteration 0: obj = {0: .5f}'.format(obj))
+
+    history = []
+    it = 0
+    diffVar = None
+    grdOld = None
+    obj_old = None
+    gval = None
+
+    def finish():
+        if hasattr(opt, 'endOfProcedure'):
+            opt.endOfProcedure()
+        elif hasattr(opt, 'endOfIteration'):
+            opt.endOfIteration()
+
+    t_iter = time.process_time()
+    while it < maxIter:
+        t0 = time.process_time()
+        if hasattr(opt, 'startOfIteration'):
+            opt.startOfIteration()
+        if opt.reset:
+            opt.obj = None
+            obj = opt.objectiveFun()
+            if verb:
+                logging.info(f'recomputed objective {obj:.5f}')
+            obj_old = None
+            gval = None
+        grd = opt.getGradient(gradCoeff) if gval is None else gval
+
+        if TestGradient:
+            dirfoo = opt.randomDir() if hasattr(opt, 'randomDir') else np.random.normal(size=np.shape(grd))
+            epsfoo = 1e-8
+            o1 = opt.updateTry(dirfoo, epsfoo, obj - 1e8)
+            o2 = opt.updateTry(dirfoo, -epsfoo, obj - 1e8)
+            [gd] = dot(grd, [dirfoo])
+            logging.info('Test Gradient: %.4f %.4f' % ((o1 - o2) / (2 * epsfoo), -gd * gradCoeff))
+
+        if not opt.reset and it > 0:
+            history.append([diffVar, addProd(grd, grdOld, -1)])
+            if len(history) > memory:
+                history.pop(0)
+            q = copyDir(grd)
+            rho, alpha = [], []
+            for s_k, y_k in reversed(history):
+                rho.append(1 / dot(y_k, [s_k])[0])
+                alpha.append(rho[-1] * dot(s_k, [q])[0])
+                q = addProd(q, y_k, -alpha[-1])
+            rho.reverse()
+            alpha.reverse()
+            s_k, y_k = history[-1]
+            c = dot(s_k, [y_k])[0] / dot(y_k, [y_k])[0]
+            if c < 1e-10:
+                c = 1
+            q = prod(q, c)
+            for k, (s_k, y_k) in enumerate(history):
+                beta = rho[k] * dot(y_k, [q])[0]
+                q = addProd(q, s_k, alpha[k] - beta)
+        else:
+            history = []
+            q = copyDir(grd)
+
+        grd2 = dot(grd, [grd])[0]
+        grdTry = np.sqrt(np.maximum(1e-20, dot(q, [q])[0]))
+        dir0 = copyDir(q)
+        t_init = 1. / grdTry if (it == 0 or opt.reset) else 1.
+        grdOld = copyDir(grd)
+
+        if it == 0 or it == burnIn:
+            if gradEps is None:
+                gradEps = max(0.001 * np.sqrt(grd2), 0.0001)
+            else:
+                gradEps = min(gradEps, 0.0001 * np.sqrt(grd2))
+            logging.info(f'Gradient threshold: {gradEps:.6f}')
+
+        if it < burnIn:
+            Wolfe = False
+            eps = epsInit
+        elif Wolfe:
+            eps = 1.
+        else:
+            eps = min(eps, epsMax / grdTry)
+
+        eps, fc, gc, phi_star, old_fval, gval = line_search(opt, dir0, gfk=grd, old_fval=obj, old_old_fval=obj_old,
+                                                            c1=1e-4, c2=0.9, amax=None, t_init=t_init, maxiter=10)
+        if eps is not None:
+            diffVar = prod(dir0, -eps)
+            obj_old = obj
+            opt.acceptVarTry()
+            obj = phi_star
+            newreset = False
+        else:
+            logging.info('Wolfe search unsuccessful')
+            if opt.reset:
+                logging.info('Cannot go any further')
+                opt.converged = False
+                finish()
+                break
+            newreset = True
+            gval = None
+
+        if obj_old is not None and np.fabs(obj - obj_old) < 1e-7 and stopCondition():
+            logging.info(f'iteration {it + 1:d}: obj = {obj:.5f}, eps = {eps:.5f}, gradient: {np.sqrt(grd2):.5f}')
+            if it > burnIn or opt.reset:
+                logging.info('Stopping Gradient Descent: small variation')
+                opt.converged = True
+                finish()
+                break
+            newreset = True
+
+        now = time.process_time()
+        if verb or it == maxIter:
+            e_s = 'None' if eps is None else f'{eps:.5f}'
+            logging.info(f'iteration {it + 1:d}: obj = {obj:.5f}, eps = {e_s}, gradient: {np.sqrt(grd2):.5f}, '
+                         f'time = {now - t0:.04f}, {now - t_iter:.04f}')
+        t_iter = now
+
+        if np.sqrt(grd2) < gradEps and stopCondition():
+            logging.info('Stopping Gradient Descent: small gradient')
+            opt.converged = True
+            finish()
+            break
+        eps = np.minimum(100 * eps, epsMax) if eps is not None else epsMax
+        opt.reset = newreset
+        if hasattr(opt, 'endOfIteration'):
+            opt.endOfIteration()
+        if not opt.reset:
+            it += 1
+
+    if it == maxIter and hasattr(opt, 'endOfProcedure'):
+        opt.endOfProcedure()
+    if hasattr(opt, 'endOptim'):
+        opt.endOptim()
+    return opt.getVariable()

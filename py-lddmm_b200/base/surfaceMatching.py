@@ -1,0 +1,294 @@
+"""Drop-in surface matching drivers with device-resident state (reference: base/surfaceMatching.py:75-1590,
+base/secondOrderSurfaceMatching.py:41, base/pointSetMatching.py, base/basicMatching.py).
+
+`SurfaceMatching` (first-order LDDMM, controls a_t, t < T) and `SecondOrderSurfaceMatching` (geodesic shooting
+from a_0) keep the reference's options dictionary, the optimiser protocol (objectiveFun, updateTry, getGradient,
+acceptVarTry, dotProduct_euclidean, addProd, prod, copyDir, randomDir, startOfIteration, endOfIteration) and
+`optimizeMatching()` (L-BFGS, memory 50, weak Wolfe). Controls, trajectories and covectors are float64 CUDA
+tensors; every kernel sum runs in the sm_100a library; the objective and the dot products are FP64 device
+reductions read back as Python floats for the line-search comparisons.
+
+Differences from the reference, by design:
+  * the trajectory computed for a line-search trial is reused by the gradient at the accepted step (the reference
+    shoots forward again inside every gradient, base/pointEvolution.py:516-519 and base/surfaceMatching.py:757);
+  * the first-order kinetic energy sum_t a_t.K(x_t)a_t is read from the shooting kernels' epilogue instead of a
+    second K(x_t)a_t per time step (base/surfaceMatching.py:546-548);
+  * affine parts, landmarks, symmetric / unreduced / SGD variants and file output are not implemented.
+"""
+import logging
+from copy import deepcopy
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from . import bfgs as _bfgs
+from . import pointEvolution as evol
+from .kernelFunctions import Kernel
+from .surfaceDistances import SurfaceDataTerm
+from .surfaces import Surface
+
+
+class Control(dict):
+    pass
+
+
+class State(dict):
+    pass
+
+
+def _make_kernel(spec, default_sigma):
+    if isinstance(spec, Kernel):
+        return spec
+    if spec is None:
+        return Kernel(name='gauss', sigma=default_sigma)
+    if isinstance(spec, (list, tuple)):
+        return Kernel(name=spec[0], sigma=spec[1])
+    raise TypeError('kernel must be a Kernel or a (name, sigma) tuple')
+
+
+class _DeviceMatching:
+    control_key = None
+
+    def getDefaultOptions(self):
+        return {'timeStep': 0.1, 'algorithm': 'bfgs', 'unreduced': False, 'Wolfe': True, 'burnIn': 10,
+                'epsInit': 1., 'KparDiff': None, 'KparDist': None, 'pk_dtype': 'float32', 'sigmaError': 1.0,
+                'errorType': 'measure', 'vfun': None, 'maxIter': 1000, 'regWeight': 1.0, 'affine': None,
+                'affineKernel': False, 'testGradient': False, 'Landmarks': None, 'saveFile': 'evolution',
+                'saveRate': 10, 'mode': 'normal', 'verb': True, 'pplot': False, 'outputDir': '.',
+                'symmetric': False, 'internalCost': None, 'lineSearch': 'Weak_Wolfe', 'gradTol': -1.,
+                'gradLB': 0.001, 'initialMomentum': None}
+
+    def __init__(self, Template=None, Target=None, options=None):
+        self.options = self.getDefaultOptions()
+        if options is not None:
+            self.options.update(options)
+        o = self.options
+        if o['affine'] not in (None, 'none'):
+            raise NotImplementedError('affine components are not implemented')
+        if o['Landmarks'] is not None or o['symmetric'] or o['unreduced'] or o['internalCost'] is not None:
+            raise NotImplementedError('landmarks / symmetric / unreduced / internal-cost variants are not implemented')
+        if o['algorithm'] not in ('bfgs',):
+            raise NotImplementedError("algorithm='bfgs' is implemented")
+        if o['mode'] == 'debug':
+            o['testGradient'] = True
+            o['pk_dtype'] = 'float64'
+        self.fv0 = Surface(surf=Template)
+        self.fv1 = Surface(surf=Target)
+        self.fvDef = Surface(surf=self.fv0)
+        self.dim = 3
+        o['KparDiff'] = _make_kernel(o['KparDiff'], 6.5)
+        o['KparDist'] = _make_kernel(o['KparDist'], 2.5)
+        self.Kdiff_dtype = o['pk_dtype']
+        self.resetPK(o['pk_dtype'])
+        kind = o['errorType']
+        if kind not in ('varifold', 'current', 'measure'):
+            raise NotImplementedError(f"errorType '{kind}' is not implemented")
+        if o['vfun'] is not None:
+            raise NotImplementedError('only the default varifold weight is implemented')
+        w0 = np.asarray(self.fv0.weights, dtype=np.float64)
+        w1 = np.asarray(self.fv1.weights, dtype=np.float64)
+        self.data = SurfaceDataTerm(self.fv0.faces, self.fv1.vertices, self.fv1.faces, o['KparDist'], kind=kind,
+                                    weights=None if np.all(w0 == 1) else w0, target_weights=None if np.all(w1 == 1)
+                                    else w1, nv=self.fv0.vertices.shape[0])
+        self.x0 = nat.as_device(self.fv0.vertices)
+        self.npt = self.x0.shape[0]
+        self.origin = nat.centroid(self.x0)
+        self.Tsize = int(round(1.0 / o['timeStep']))
+        self.sigma2 = o['sigmaError'] ** 2
+        self.euclideanGradient = True
+        self.gradCoeff = 1.
+        self.gradEps = o['gradTol']
+        self.burnIn = o['burnIn']
+        self.obj = None
+        self.objTry = None
+        self.reset = False
+        self.iter = 0
+        self.pkBuffer = 0
+        self.history = []
+        self.control = Control()
+        self.controlTry = Control()
+        self.state = State()
+        self.stateTry = None
+        self.initialize_variables()
+
+    # ------------------------------------------------------------------ precision switching
+    def resetPK(self, newType=None):
+        t = self.Kdiff_dtype if newType is None else newType
+        self.options['KparDiff'].pk_dtype = t
+        self.options['KparDist'].pk_dtype = t
+        if hasattr(self, 'data'):
+            self.data.precision = nat.FP64 if t == 'float64' else nat.FP32C
+        self.pkBuffer = 0
+
+    def startOfIteration(self):
+        if self.reset:
+            logging.info('switching to float64')
+            self.resetPK('float64')
+
+    # ------------------------------------------------------------------ data term
+    def dataTerm(self, xdef):
+        return self.data.energy(xdef)[0] / self.sigma2
+
+    def endPointGradient(self, xdef):
+        return self.data.gradient(xdef) / self.sigma2
+
+    # ------------------------------------------------------------------ optimiser protocol
+    def getVariable(self):
+        return self.control
+
+    def objectiveFun(self):
+        if self.obj is None:
+            self.obj0 = self.data.norm0() / self.sigma2
+            objDef, self.state = self.objectiveFunDef(self.control, withTrajectory=True)
+            self.obj = float(self.obj0 + objDef + self.dataTerm(self.state['xt'][-1]))
+        return self.obj
+
+    def updateTry(self, dr, eps, objRef=None):
+        controlTry = Control()
+        for k, v in dr.items():
+            if v is not None and self.control.get(k) is not None:
+                controlTry[k] = self.control[k] - eps * v
+        objDef, st = self.objectiveFunDef(controlTry, withTrajectory=True)
+        objTry = float(self.obj0 + objDef + self.dataTerm(st['xt'][-1]))
+        if np.isnan(objTry):
+            return 1e500
+        if objRef is None or objTry < objRef:
+            self.controlTry = controlTry
+            self.stateTry = st
+            self.objTry = objTry
+        return objTry
+
+    def acceptVarTry(self):
+        self.obj = self.objTry
+        self.control = self.controlTry
+        self.state = self.stateTry
+
+    def setUpdate(self, update):
+        control = Control()
+        for k, v in update[0].items():
+            if v is not None and self.control.get(k) is not None:
+                control[k] = self.control[k] - update[1] * v
+        _, st = self.objectiveFunDef(control, withTrajectory=True)
+        return control, st
+
+    def dotProduct_euclidean(self, g1, g2):
+        keys = [k for k in g1 if g1[k] is not None]
+        vals = [sum((g1[k] * gr[k]).sum() for k in keys if gr.get(k) is not None) for gr in g2]
+        return torch.stack([torch.as_tensor(v, dtype=torch.float64, device=self.x0.device) for v in vals]).tolist()
+
+    dotProduct = dotProduct_euclidean
+
+    def addProd(self, dir1, dir2, beta):
+        return Control({k: dir1[k] + beta * dir2[k] for k in dir1 if dir1[k] is not None and dir2.get(k) is not None})
+
+    def prod(self, dir1, beta):
+        return Control({k: beta * v for k, v in dir1.items() if v is not None})
+
+    def copyDir(self, dir0):
+        return Control({k: (v.clone() if isinstance(v, torch.Tensor) else deepcopy(v)) for k, v in dir0.items()})
+
+    def endOfIteration(self, endP=False):
+        self.iter += 1
+        self.history.append(self.obj)
+        if self.pkBuffer > 50:
+            self.resetPK()
+        else:
+            self.pkBuffer += 1
+
+    def endOfProcedure(self):
+        self.endOfIteration(endP=True)
+
+    def endOptim(self):
+        self.fvDef.updateVertices(self.state['xt'][-1].cpu().numpy())
+
+    def optimizeMatching(self):
+        grd = self.getGradient(self.gradCoeff)
+        [grd2] = self.dotProduct_euclidean(grd, [grd])
+        if self.gradEps < 0:
+            self.gradEps = max(1e-5, np.sqrt(grd2) / 10000)
+        self.epsMax = 5.
+        logging.info(f'Gradient lower bound: {self.gradEps:.5f}')
+        _bfgs.bfgs(self, verb=self.options['verb'], maxIter=self.options['maxIter'],
+                   TestGradient=self.options['testGradient'], epsInit=self.options['epsInit'],
+                   Wolfe=self.options['Wolfe'], lineSearch=self.options['lineSearch'], memory=50)
+        return self.control
+
+
+class SurfaceMatching(_DeviceMatching):
+    """First-order LDDMM surface matching (base/surfaceMatching.py:75)."""
+    control_key = 'at'
+
+    def initialize_variables(self):
+        self.control['at'] = torch.zeros((self.Tsize, self.npt, 3), dtype=torch.float64, device=self.x0.device)
+        self.control['Afft'] = None
+        self.state['xt'] = self.x0.unsqueeze(0).repeat(self.Tsize + 1, 1, 1)
+
+    def objectiveFunDef(self, control, var=None, withTrajectory=True, withJacobian=False):
+        """sum_t regWeight dt a_t.K(x_t)a_t with the trajectory (base/surfaceMatching.py:468-565)."""
+        e = torch.zeros(1, dtype=torch.float64, device=self.x0.device)
+        xt = evol.shoot_first_order(self.x0, control['at'], self.options['KparDiff'],
+                                    regweight=self.options['regWeight'], energy=e, origin=self.origin)
+        st = State(xt=xt)
+        return (e[0], st) if withTrajectory or withJacobian else e[0]
+
+    def getGradient(self, coeff=1.0, update=None):
+        """(base/surfaceMatching.py:1040-1105, euclidean gradient K(x_t)(2 w a_t - p_{t+1}) / (coeff T))."""
+        if update is None:
+            control, st = self.control, self.state
+        else:
+            control, st = self.setUpdate(update)
+        px1 = -self.endPointGradient(st['xt'][-1])
+        _, dat = evol.first_order_gradient(st['xt'], control['at'], px1, self.options['KparDiff'],
+                                           self.options['regWeight'], euclidean=self.euclideanGradient,
+                                           origin=self.origin)
+        grd = Control()
+        grd['at'] = dat / (coeff * self.Tsize)
+        return grd
+
+    def randomDir(self):
+        return Control(at=torch.randn((self.Tsize, self.npt, 3), dtype=torch.float64, device=self.x0.device))
+
+
+class SecondOrderSurfaceMatching(_DeviceMatching):
+    """Geodesic-shooting surface matching (base/secondOrderSurfaceMatching.py:41,
+    base/secondOrderPointSetMatching.py:45-494)."""
+    control_key = 'a0'
+
+    def initialize_variables(self):
+        a0 = self.options['initialMomentum']
+        if a0 is None:
+            self.control['a0'] = torch.zeros((self.npt, 3), dtype=torch.float64, device=self.x0.device)
+        else:
+            self.control['a0'] = nat.as_device(a0).clone()
+        self.control['Afft'] = None
+        xt, at = evol.shoot_second_order(self.x0, self.control['a0'], self.options['KparDiff'],
+                                         self.options['timeStep'], origin=self.origin)
+        self.state = State(xt=xt, at=at)
+
+    def objectiveFunDef(self, control, var=None, withTrajectory=True, withJacobian=False):
+        """0.5 a0.K(x0)a0 with the geodesic trajectory (base/secondOrderPointSetMatching.py:113-148)."""
+        K = self.options['KparDiff']
+        a0 = control['a0']
+        xt, at = evol.shoot_second_order(self.x0, a0, K, self.options['timeStep'], origin=self.origin)
+        obj = 0.5 * (a0 * K._apply_k(self.x0, self.x0, a0, float(np.asarray(K.sigma).ravel()[0]), self.origin)).sum() \
+            if np.asarray(K.sigma).size == 1 else 0.5 * (a0 * K.applyK(self.x0, a0)).sum()
+        st = State(xt=xt, at=at)
+        return (obj, st) if withTrajectory or withJacobian else obj
+
+    def getGradient(self, coeff=1.0, update=None):
+        """da0 = K(x0)a0 - pa_0 after the adjoint sweep (base/secondOrderPointSetMatching.py:379-483)."""
+        if update is None:
+            control, st = self.control, self.state
+        else:
+            control, st = self.setUpdate(update)
+        px1 = -self.endPointGradient(st['xt'][-1])
+        pa1 = torch.zeros_like(px1)
+        _, _, da0 = evol.second_order_adjoint(st['xt'], st['at'], px1, pa1, self.options['KparDiff'],
+                                              self.options['timeStep'], origin=self.origin)
+        grd = Control()
+        grd['a0'] = da0 / coeff
+        return grd
+
+    def randomDir(self):
+        return Control(a0=torch.randn((self.npt, 3), dtype=torch.float64, device=self.x0.device))

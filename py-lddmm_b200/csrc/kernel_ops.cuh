@@ -1,19 +1,28 @@
 // Pair functors of the Gaussian kernel operators (one width sigma, KP = -1).
 //
 // Notation: y' = (y - o) s, x' = (x - o) s, d = y'_k - x'_l, e = expneg(|d|^2) = exp(-|y_k-x_l|^2/(2 sigma^2)),
-// kappa = 1/(s sigma^2) so that (y_k - x_l)/sigma^2 = kappa d. Per-pair FP32/SFU work is listed per op
-// (the figures used for the roofline).
+// kappa = 1/(s sigma^2) so that (y_k - x_l)/sigma^2 = kappa d. Each functor is written once for V = F2 (two FP32
+// targets per packed instruction) and V = double. Per-pair FP32 lane-op / SFU counts are listed per op (the
+// figures used for the roofline; a packed instruction counts as two lane-ops).
 #pragma once
 #include "lddmm_common.cuh"
 
 namespace lddmm {
 
+template <typename V>
+__device__ __forceinline__ V sqdist(V d0, V d1, V d2) {
+  return fma(d2, d2, fma(d1, d1, d0 * d0));
+}
+template <typename V>
+__device__ __forceinline__ V dot3(V a0, V a1, V a2, V b0, V b1, V b2) {
+  return fma(a2, b2, fma(a1, b1, a0 * b0));
+}
+
 // K(y, x) a  -- base/kernelFunctions_util.py:451-466. 9 FP32 + 1 SFU per pair.
 // Epilogue (used by the shooting drivers): out = base_sign * base + scale * K a, and optionally
 // dots[i] = dotw_i . (K a)_i for FP64 energy reductions.
-template <typename R>
 struct OpK {
-  static constexpr int NV = 2, NA = 3;
+  static constexpr int NS = 6, NA = 3;
   struct Params {
     const double *y, *x, *a;
     double* out;
@@ -24,22 +33,24 @@ struct OpK {
     const double* dotw = nullptr;
     double* dots = nullptr;
   };
-  struct Tgt { R y0, y1, y2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.y, i, P.f, t.y0, t.y1, t.y2);
+  template <typename V> struct Tgt { V y0, y1, y2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.y, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.y, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.y, i0, i1, 2, P.f.o2, P.f.s);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
-    s[0].w = R(0);
-    s[1].w = R(0);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    f[3] = P.a[3 * l]; f[4] = P.a[3 * l + 1]; f[5] = P.a[3 * l + 2];
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    acc[0] += e * s[1].x;
-    acc[1] += e * s[1].y;
-    acc[2] += e * s[1].z;
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    acc[0] = fma(e, s[3], acc[0]);
+    acc[1] = fma(e, s[4], acc[1]);
+    acc[2] = fma(e, s[5], acc[2]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     if (P.dots)
@@ -54,48 +65,54 @@ struct OpK {
 };
 
 // DK^T(y, x; p, a) -- base/kernelFunctions_util.py:773-793 with gauss_fun_diffT (:233).
-//   mode 0 (plain): c = p_k.a_l                         13 FP32 + 1 SFU
-//   mode 1 (sym)  : c = p_k.a_l + a_k.p_l               16 FP32 + 1 SFU
-//   mode 2 (lddmm): c = p_k.a_l + a_k.(p_l - 2 w a_l)   16 FP32 + 1 SFU (source-side q_l precomputed)
+//   MODE 0 (plain): c = p_k.a_l                         13 FP32 + 1 SFU
+//   MODE 1 (sym)  : c = p_k.a_l + a_k.p_l               16 FP32 + 1 SFU
+//   MODE 2 (lddmm): c = p_k.a_l + a_k.(p_l - 2 w a_l)   16 FP32 + 1 SFU (source-side q_l precomputed)
 // out_k = -kappa sum_l e c d.
-template <typename R, int MODE>
+template <int MODE>
 struct OpDiffKT {
-  static constexpr int NV = (MODE == 0) ? 2 : 3, NA = 3;
+  static constexpr int NS = (MODE == 0) ? 6 : 9, NA = 3;
   struct Params {
     const double *y, *x, *p, *a;  // p: (n,3) target-indexed (and source-indexed for sym/lddmm), a: (m,3)
     double* out;
     Frame f;
     double w;  // regweight (lddmm)
   };
-  struct Tgt { R y0, y1, y2, p0, p1, p2, a0, a1, a2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.y, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.p, i, t.p0, t.p1, t.p2);
-    if (MODE != 0) load_vec(P.a, i, t.a0, t.a1, t.a2);
-    else { t.a0 = t.a1 = t.a2 = R(0); }
-  }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
-    s[0].w = R(0);
-    s[1].w = R(0);
+  template <typename V> struct Tgt { V y0, y1, y2, p0, p1, p2, a0, a1, a2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.y, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.y, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.y, i0, i1, 2, P.f.o2, P.f.s);
+    t.p0 = tgt_field<V>(P.p, 3, i0, i1, 0);
+    t.p1 = tgt_field<V>(P.p, 3, i0, i1, 1);
+    t.p2 = tgt_field<V>(P.p, 3, i0, i1, 2);
     if (MODE != 0) {
-      const double k = (MODE == 2) ? 2.0 * P.w : 0.0;
-      s[2].x = (R)(P.p[3 * l + 0] - k * P.a[3 * l + 0]);
-      s[2].y = (R)(P.p[3 * l + 1] - k * P.a[3 * l + 1]);
-      s[2].z = (R)(P.p[3 * l + 2] - k * P.a[3 * l + 2]);
-      s[2].w = R(0);
+      t.a0 = tgt_field<V>(P.a, 3, i0, i1, 0);
+      t.a1 = tgt_field<V>(P.a, 3, i0, i1, 1);
+      t.a2 = tgt_field<V>(P.a, 3, i0, i1, 2);
+    } else {
+      t.a0 = t.a1 = t.a2 = VT<V>::zero();
     }
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    R c = t.p0 * s[1].x + t.p1 * s[1].y + t.p2 * s[1].z;
-    if (MODE != 0) c += t.a0 * s[2].x + t.a1 * s[2].y + t.a2 * s[2].z;
-    const R ec = e * c;
-    acc[0] += ec * d0;
-    acc[1] += ec * d1;
-    acc[2] += ec * d2;
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    for (int c = 0; c < 3; ++c) f[3 + c] = P.a[3 * l + c];
+    if (MODE != 0) {
+      const double k = (MODE == 2) ? 2.0 * P.w : 0.0;
+      for (int c = 0; c < 3; ++c) f[6 + c] = P.p[3 * l + c] - k * P.a[3 * l + c];
+    }
+  }
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    V c = dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]);
+    if (MODE != 0) c = fma(t.a0, s[6], fma(t.a1, s[7], fma(t.a2, s[8], c)));
+    const V ec = e * c;
+    acc[0] = fma(ec, d0, acc[0]);
+    acc[1] = fma(ec, d1, acc[1]);
+    acc[2] = fma(ec, d2, acc[2]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = -P.f.kappa;
@@ -109,40 +126,47 @@ struct OpDiffKT {
 // out_k = sum_l (n_k.a_l) e [ (D.Dp) D / sigma^4 - Dp / sigma^2 ],  D = x_k - x_l, Dp = p_k - p_l
 //       = kappa^2 A_k - (p_k B_k - C_k)/sigma^2 with A = sum c e (d.Dp) d, B = sum c e, C = sum c e p_l.
 // 24 FP32 + 1 SFU per pair.
-template <typename R>
 struct OpDDiffK {
-  static constexpr int NV = 3, NA = 7;
+  static constexpr int NS = 9, NA = 7;
   struct Params {
     const double *x, *nn, *a, *p;
     double* out;
     Frame f;
   };
-  struct Tgt { R y0, y1, y2, n0, n1, n2, p0, p1, p2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.x, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.nn, i, t.n0, t.n1, t.n2);
-    load_vec(P.p, i, t.p0, t.p1, t.p2);
+  template <typename V> struct Tgt { V y0, y1, y2, n0, n1, n2, p0, p1, p2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.n0 = tgt_field<V>(P.nn, 3, i0, i1, 0);
+    t.n1 = tgt_field<V>(P.nn, 3, i0, i1, 1);
+    t.n2 = tgt_field<V>(P.nn, 3, i0, i1, 2);
+    t.p0 = tgt_field<V>(P.p, 3, i0, i1, 0);
+    t.p1 = tgt_field<V>(P.p, 3, i0, i1, 1);
+    t.p2 = tgt_field<V>(P.p, 3, i0, i1, 2);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
-    load_vec(P.p, l, s[2].x, s[2].y, s[2].z);
-    s[0].w = s[1].w = s[2].w = R(0);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    for (int c = 0; c < 3; ++c) {
+      f[3 + c] = P.a[3 * l + c];
+      f[6 + c] = P.p[3 * l + c];
+    }
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    const R q0 = t.p0 - s[2].x, q1 = t.p1 - s[2].y, q2 = t.p2 - s[2].z;
-    const R dq = d0 * q0 + d1 * q1 + d2 * q2;
-    const R ce = e * (t.n0 * s[1].x + t.n1 * s[1].y + t.n2 * s[1].z);
-    const R ced = ce * dq;
-    acc[0] += ced * d0;
-    acc[1] += ced * d1;
-    acc[2] += ced * d2;
-    acc[3] += ce;
-    acc[4] += ce * s[2].x;
-    acc[5] += ce * s[2].y;
-    acc[6] += ce * s[2].z;
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V dq = dot3(d0, d1, d2, t.p0 - s[6], t.p1 - s[7], t.p2 - s[8]);
+    const V ce = e * dot3(t.n0, t.n1, t.n2, s[3], s[4], s[5]);
+    const V ced = ce * dq;
+    acc[0] = fma(ced, d0, acc[0]);
+    acc[1] = fma(ced, d1, acc[1]);
+    acc[2] = fma(ced, d2, acc[2]);
+    acc[3] = acc[3] + ce;
+    acc[4] = fma(ce, s[6], acc[4]);
+    acc[5] = fma(ce, s[7], acc[5]);
+    acc[6] = fma(ce, s[8], acc[6]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k2 = P.f.kappa * P.f.kappa, is2 = P.f.inv_s2;
@@ -153,33 +177,38 @@ struct OpDDiffK {
 
 // DK_{1and2}(x; a1, a2) -- base/kernelFunctions_util.py:672-675 with gauss_fun_diff (:195).
 // out_k = sum_l -(D.(a1_k - a1_l))/sigma^2 e a2_l = -kappa sum_l (d.(a1_k - a1_l)) e a2_l. 16 FP32 + 1 SFU.
-template <typename R>
 struct OpDiffK1and2 {
-  static constexpr int NV = 3, NA = 3;
+  static constexpr int NS = 9, NA = 3;
   struct Params {
     const double *x, *a1, *a2;
     double* out;
     Frame f;
   };
-  struct Tgt { R y0, y1, y2, b0, b1, b2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.x, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.a1, i, t.b0, t.b1, t.b2);
+  template <typename V> struct Tgt { V y0, y1, y2, b0, b1, b2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.b0 = tgt_field<V>(P.a1, 3, i0, i1, 0);
+    t.b1 = tgt_field<V>(P.a1, 3, i0, i1, 1);
+    t.b2 = tgt_field<V>(P.a1, 3, i0, i1, 2);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a1, l, s[1].x, s[1].y, s[1].z);
-    load_vec(P.a2, l, s[2].x, s[2].y, s[2].z);
-    s[0].w = s[1].w = s[2].w = R(0);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    for (int c = 0; c < 3; ++c) {
+      f[3 + c] = P.a1[3 * l + c];
+      f[6 + c] = P.a2[3 * l + c];
+    }
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    const R g = d0 * (t.b0 - s[1].x) + d1 * (t.b1 - s[1].y) + d2 * (t.b2 - s[1].z);
-    const R eg = e * g;
-    acc[0] += eg * s[2].x;
-    acc[1] += eg * s[2].y;
-    acc[2] += eg * s[2].z;
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V eg = e * dot3(d0, d1, d2, t.b0 - s[3], t.b1 - s[4], t.b2 - s[5]);
+    acc[0] = fma(eg, s[6], acc[0]);
+    acc[1] = fma(eg, s[7], acc[1]);
+    acc[2] = fma(eg, s[8], acc[2]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = -P.f.kappa;
@@ -190,28 +219,30 @@ struct OpDiffK1and2 {
 };
 
 // Divergence: out_k = sum_l -((y_k - x_l).a_l)/sigma^2 e = -kappa sum_l (d.a_l) e
-// (base/kernelFunctions_util.py:611-626 applyDiv with gauss_fun_diff). 11 FP32 + 1 SFU.
-template <typename R>
+// (base/kernelFunctions_util.py:611-626 applyDiv with gauss_fun_diff). 10 FP32 + 1 SFU.
 struct OpDiv {
-  static constexpr int NV = 2, NA = 1;
+  static constexpr int NS = 6, NA = 1;
   struct Params {
     const double *y, *x, *a;
     double* out;
     Frame f;
   };
-  struct Tgt { R y0, y1, y2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.y, i, P.f, t.y0, t.y1, t.y2);
+  template <typename V> struct Tgt { V y0, y1, y2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.y, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.y, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.y, i0, i1, 2, P.f.o2, P.f.s);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
-    s[0].w = s[1].w = R(0);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    f[3] = P.a[3 * l]; f[4] = P.a[3 * l + 1]; f[5] = P.a[3 * l + 2];
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    acc[0] += e * (d0 * s[1].x + d1 * s[1].y + d2 * s[1].z);
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    acc[0] = fma(e, dot3(d0, d1, d2, s[3], s[4], s[5]), acc[0]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     P.out[i] = -P.f.kappa * acc[0];
@@ -220,31 +251,35 @@ struct OpDiv {
 
 // K-tensor: out_k = sum_l e (ay_k ax_l + (by_k.bx_l)^2) (base/kernelFunctions_util.py:1475-1506).
 // Accumulates A = sum e ax_l and B = sum e g^2 so that ay_k multiplies once per target. 13 FP32 + 1 SFU.
-template <typename R>
 struct OpKTensor {
-  static constexpr int NV = 2, NA = 2;
+  static constexpr int NS = 7, NA = 2;
   struct Params {
     const double *y, *x, *ay, *ax, *by, *bx;
     double* out;
     Frame f;
   };
-  struct Tgt { R y0, y1, y2, b0, b1, b2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.y, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.by, i, t.b0, t.b1, t.b2);
+  template <typename V> struct Tgt { V y0, y1, y2, b0, b1, b2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.y, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.y, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.y, i0, i1, 2, P.f.o2, P.f.s);
+    t.b0 = tgt_field<V>(P.by, 3, i0, i1, 0);
+    t.b1 = tgt_field<V>(P.by, 3, i0, i1, 1);
+    t.b2 = tgt_field<V>(P.by, 3, i0, i1, 2);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    s[0].w = (R)P.ax[l];
-    load_vec(P.bx, l, s[1].x, s[1].y, s[1].z);
-    s[1].w = R(0);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    f[3] = P.ax[l];
+    f[4] = P.bx[3 * l]; f[5] = P.bx[3 * l + 1]; f[6] = P.bx[3 * l + 2];
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    const R g = t.b0 * s[1].x + t.b1 * s[1].y + t.b2 * s[1].z;
-    acc[0] += e * s[0].w;
-    acc[1] += e * (g * g);
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V g = dot3(t.b0, t.b1, t.b2, s[4], s[5], s[6]);
+    acc[0] = fma(e, s[3], acc[0]);
+    acc[1] = fma(e, g * g, acc[1]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     P.out[i] = P.ay[i] * acc[0] + acc[1];

@@ -1,5 +1,5 @@
 // C-ABI entry points of the Gaussian kernel operators (Kernel.applyK / applyDiffKT / applyDDiffK11and12 /
-// applyDiffK1and2 / applyDivergence / applyKTensor and the dense-weight variants).
+// applyDiffK1and2 / applyDivergence / applyKTensor).
 #include "../../include/lddmm_b200.h"
 #include "kernel_ops.cuh"
 #include "launch_config.cuh"
@@ -7,11 +7,25 @@
 namespace lddmm {
 
 int device_sm_count() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
-  int sms = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 148;
+  static int cached = 0;
+  if (cached > 0) return cached;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+    cudaGetLastError();
+    return 148;
+  }
+  cached = sms;
   return sms;
+}
+
+int resident_ctas(const void* kernel, int threads) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
 }
 
 __global__ void ordered_sum_kernel(const double* __restrict__ v, int count, double scale, double* out,
@@ -32,42 +46,41 @@ namespace {
 
 bool bad_ptr(const void* p, int64_t count) { return count > 0 && p == nullptr; }
 
-template <template <typename> class OpT, int TPB32, int RT32, int TPB64, int RT64, class Fill>
+template <class Op, int TPB32, int RT32, class Fill>
 int dispatch(int precision, int64_t n, int64_t m, double sigma, const double* origin, void* ws, size_t wsb,
              cudaStream_t st, Fill fill) {
+  typename Op::Params P;
   if (precision == kFP32Compensated) {
-    typename OpT<float>::Params P;
-    P.f = make_frame(origin, sigma, PT<float>::kScale);
+    P.f = make_frame(origin, sigma, VT<F2>::kScale);
     fill(P);
-    return run_pairs<OpT<float>, float, TPB32, RT32>(P, n, m, ws, wsb, st, kCtasPerSm);
+    return run_pairs<Op, F2, TPB32, RT32>(P, n, m, ws, wsb, st);
   } else if (precision == kFP64) {
-    typename OpT<double>::Params P;
-    P.f = make_frame(origin, sigma, PT<double>::kScale);
+    P.f = make_frame(origin, sigma, VT<double>::kScale);
     fill(P);
-    return run_pairs<OpT<double>, double, TPB64, RT64>(P, n, m, ws, wsb, st, kCtasPerSm);
+    return run_pairs<Op, double, kTpb64, kRt64>(P, n, m, ws, wsb, st);
   }
   return kInvalidArgument;
 }
 
-template <typename R> using OpDiffKT0 = OpDiffKT<R, 0>;
-template <typename R> using OpDiffKT1 = OpDiffKT<R, 1>;
-template <typename R> using OpDiffKT2 = OpDiffKT<R, 2>;
+template <class Op, int TPB32, int RT32>
+size_t op_ws(int64_t n, int64_t m, int precision) {
+  return precision == kFP32Compensated ? pairs_ws_bytes<Op, F2, TPB32, RT32>(n, m)
+                                       : pairs_ws_bytes<Op, double, kTpb64, kRt64>(n, m);
+}
 
 }  // namespace
 
 size_t kernel_sums_ws_bytes(int64_t n, int64_t m, int precision) {
   size_t b = 0;
   auto upd = [&](size_t v) { b = v > b ? v : b; };
-  if (precision == kFP32Compensated) {
-    upd(pairs_ws_bytes<OpK<float>, float, kTpbLight, kRtLight>(n, m, kCtasPerSm));
-    upd(pairs_ws_bytes<OpDiffKT<float, 2>, float, kTpbLight, kRtLight>(n, m, kCtasPerSm));
-    upd(pairs_ws_bytes<OpDDiffK<float>, float, kTpbHeavy, kRtHeavy>(n, m, kCtasPerSm));
-    upd(pairs_ws_bytes<OpDiffK1and2<float>, float, kTpbLight, kRtLight>(n, m, kCtasPerSm));
-    upd(pairs_ws_bytes<OpKTensor<float>, float, kTpbLight, kRtLight>(n, m, kCtasPerSm));
-  } else {
-    upd(pairs_ws_bytes<OpK<double>, double, kTpb64, kRt64>(n, m, kCtasPerSm));
-    upd(pairs_ws_bytes<OpDDiffK<double>, double, kTpb64, kRt64>(n, m, kCtasPerSm));
-  }
+  upd(op_ws<OpK, kTpbLight, kRtLight>(n, m, precision));
+  upd(op_ws<OpDiffKT<0>, kTpbLight, kRtLight>(n, m, precision));
+  upd(op_ws<OpDiffKT<1>, kTpbLight, kRtLight>(n, m, precision));
+  upd(op_ws<OpDiffKT<2>, kTpbLight, kRtLight>(n, m, precision));
+  upd(op_ws<OpDDiffK, kTpbHeavy, kRtHeavy>(n, m, precision));
+  upd(op_ws<OpDiffK1and2, kTpbLight, kRtLight>(n, m, precision));
+  upd(op_ws<OpDiv, kTpbLight, kRtLight>(n, m, precision));
+  upd(op_ws<OpKTensor, kTpbLight, kRtLight>(n, m, precision));
   return b;
 }
 
@@ -81,10 +94,8 @@ int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, 
                   const double* origin, double* out, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(x, m) || bad_ptr(a, m))
     return kInvalidArgument;
-  return dispatch<OpK, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, m, sigma, origin, ws, wsb,
-                                                             (cudaStream_t)stream, [&](auto& P) {
-    P.y = y; P.x = x; P.a = a; P.out = out;
-  });
+  return dispatch<OpK, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, (cudaStream_t)stream,
+                                            [&](OpK::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });
 }
 
 int lddmm_apply_diff_kt(const double* y, int64_t n, const double* x, const double* p, const double* a, int64_t m,
@@ -96,9 +107,9 @@ int lddmm_apply_diff_kt(const double* y, int64_t n, const double* x, const doubl
   if (mode != 0 && n != m) return kInvalidArgument;
   auto fill = [&](auto& P) { P.y = y; P.x = x; P.p = p; P.a = a; P.out = out; P.w = regweight; };
   cudaStream_t st = (cudaStream_t)stream;
-  if (mode == 0) return dispatch<OpDiffKT0, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, m, sigma, origin, ws, wsb, st, fill);
-  if (mode == 1) return dispatch<OpDiffKT1, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, m, sigma, origin, ws, wsb, st, fill);
-  return dispatch<OpDiffKT2, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, m, sigma, origin, ws, wsb, st, fill);
+  if (mode == 0) return dispatch<OpDiffKT<0>, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, st, fill);
+  if (mode == 1) return dispatch<OpDiffKT<1>, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, st, fill);
+  return dispatch<OpDiffKT<2>, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, st, fill);
 }
 
 int lddmm_apply_ddiff_k11and12(const double* x, const double* nn, const double* a, const double* p, int64_t n,
@@ -107,10 +118,10 @@ int lddmm_apply_ddiff_k11and12(const double* x, const double* nn, const double* 
   if (n < 0 || bad_sigma(sigma) || bad_ptr(x, n) || bad_ptr(nn, n) || bad_ptr(a, n) || bad_ptr(p, n) ||
       bad_ptr(out, n))
     return kInvalidArgument;
-  return dispatch<OpDDiffK, kTpbHeavy, kRtHeavy, kTpb64, kRt64>(precision, n, n, sigma, origin, ws, wsb,
-                                                                  (cudaStream_t)stream, [&](auto& P) {
-    P.x = x; P.nn = nn; P.a = a; P.p = p; P.out = out;
-  });
+  return dispatch<OpDDiffK, kTpbHeavy, kRtHeavy>(precision, n, n, sigma, origin, ws, wsb, (cudaStream_t)stream,
+                                                 [&](OpDDiffK::Params& P) {
+                                                   P.x = x; P.nn = nn; P.a = a; P.p = p; P.out = out;
+                                                 });
 }
 
 int lddmm_apply_diff_k1and2(const double* x, const double* a1, const double* a2, int64_t n, double sigma,
@@ -118,10 +129,10 @@ int lddmm_apply_diff_k1and2(const double* x, const double* a1, const double* a2,
                             lddmm_stream_t stream) {
   if (n < 0 || bad_sigma(sigma) || bad_ptr(x, n) || bad_ptr(a1, n) || bad_ptr(a2, n) || bad_ptr(out, n))
     return kInvalidArgument;
-  return dispatch<OpDiffK1and2, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, n, sigma, origin, ws, wsb,
-                                                                      (cudaStream_t)stream, [&](auto& P) {
-    P.x = x; P.a1 = a1; P.a2 = a2; P.out = out;
-  });
+  return dispatch<OpDiffK1and2, kTpbLight, kRtLight>(precision, n, n, sigma, origin, ws, wsb, (cudaStream_t)stream,
+                                                     [&](OpDiffK1and2::Params& P) {
+                                                       P.x = x; P.a1 = a1; P.a2 = a2; P.out = out;
+                                                     });
 }
 
 int lddmm_apply_divergence(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
@@ -129,10 +140,8 @@ int lddmm_apply_divergence(const double* y, int64_t n, const double* x, const do
                            lddmm_stream_t stream) {
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(x, m) || bad_ptr(a, m))
     return kInvalidArgument;
-  return dispatch<OpDiv, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, m, sigma, origin, ws, wsb,
-                                                               (cudaStream_t)stream, [&](auto& P) {
-    P.y = y; P.x = x; P.a = a; P.out = out;
-  });
+  return dispatch<OpDiv, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, (cudaStream_t)stream,
+                                              [&](OpDiv::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });
 }
 
 int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m, const double* ay, const double* ax,
@@ -141,10 +150,11 @@ int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m,
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(ay, n) || bad_ptr(by, n) || bad_ptr(out, n) ||
       bad_ptr(x, m) || bad_ptr(ax, m) || bad_ptr(bx, m))
     return kInvalidArgument;
-  return dispatch<OpKTensor, kTpbLight, kRtLight, kTpb64, kRt64>(precision, n, m, sigma, origin, ws, wsb,
-                                                                   (cudaStream_t)stream, [&](auto& P) {
-    P.y = y; P.x = x; P.ay = ay; P.ax = ax; P.by = by; P.bx = bx; P.out = out;
-  });
+  return dispatch<OpKTensor, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, (cudaStream_t)stream,
+                                                  [&](OpKTensor::Params& P) {
+                                                    P.y = y; P.x = x; P.ay = ay; P.ax = ax; P.by = by; P.bx = bx;
+                                                    P.out = out;
+                                                  });
 }
 
 }  // extern "C"

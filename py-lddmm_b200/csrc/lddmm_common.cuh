@@ -2,18 +2,21 @@
 //
 // Every hot operator of the point-set path is a map-reduce over (target k, source l) pairs:
 //     out_k = epilogue_k( sum_l pair(target_k, source_l) ).
-// The pair loop is FP32-FMA / MUFU bound (arithmetic intensity >> 100 flop/byte), so the design is an
-// N-body tiling: a CTA owns TPB*RT targets held in registers (RT per thread), streams tiles of TPB sources
-// through shared memory (every thread reads the same source record -> broadcast LDS.128), and the source
-// range is split into S chunks along gridDim.y so that even mid-size problems fill all 148 SMs.
+// The pair loop is FP32-pipe / MUFU bound (arithmetic intensity >> 100 flop/byte), so the design is an N-body
+// tiling: a CTA owns TPB*RT targets held in registers (RT per thread), streams tiles of TPB sources through
+// shared memory (all threads of a warp read the same source record: broadcast LDS.128), and the source range is
+// split into S chunks along gridDim.y so that mid-size problems fill all 148 SMs.
 //
-// Precision (FP32 path): coordinates are centred on a caller-given origin and pre-scaled by
-// s = sqrt(log2(e)/2)/sigma so that exp(-|y-x|^2 / (2 sigma^2)) = 2^-(|y'-x'|^2) is one `ex2.approx.ftz`.
-// Each tile is summed in plain FP32; tile sums are merged into a (hi, lo) pair by a two-sum (compensated
-// accumulation across tiles). Chunk partials (hi, lo) are reduced in FP64, in fixed order, by the
-// epilogue kernel, which also applies the per-target constants and writes float64 outputs (and, for the
-// shooting steps, the float64 Euler update of the state).
-// FP64 path ("faithful" baseline): same kernels instantiated with double, exp() and plain FP64 sums.
+// FP32 path: the pair arithmetic runs on Blackwell's packed FP32 instructions (fma/add/sub/mul .f32x2): one
+// instruction evaluates the same source against TWO targets of the thread, halving the issue slots of the FP32
+// work. Source fields are stored duplicated ((f, f) pairs) in shared memory so that a 16-byte LDS yields two
+// ready-to-use packed operands. Coordinates are centred on a caller-given origin and pre-scaled by
+// s = sqrt(log2(e)/2)/sigma so that exp(-|y-x|^2/(2 sigma^2)) = 2^-(|y'-x'|^2), one `ex2.approx.ftz` (MUFU)
+// per pair. Each tile is summed in plain FP32; tile sums are merged into a (hi, lo) pair by a two-sum
+// (compensated accumulation across tiles). Chunk partials are reduced in FP64, in fixed order, by the epilogue
+// kernel, which applies the per-target constants and writes float64 outputs (and, for shooting steps, the
+// float64 Euler update of the state).
+// FP64 path (the faithful baseline): the same pair functors instantiated with double, exp() and FP64 sums.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -32,53 +35,111 @@ enum Status : int {
 
 enum Precision : int { kFP32Compensated = 0, kFP64 = 1 };
 
-template <typename R>
-struct alignas(4 * sizeof(R)) V4 {
-  R x, y, z, w;
+// ---------------------------------------------------------------------------------------------------------
+// Packed FP32 pair (two lanes in one 64-bit register pair) and its arithmetic (PTX .f32x2, sm_100a).
+// ---------------------------------------------------------------------------------------------------------
+struct F2 {
+  unsigned long long v;
 };
 
-template <typename R> struct PT;
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void split(F2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+__device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
+__device__ __forceinline__ F2 operator-(F2 a) { return f2(0.f, 0.f) - a; }
 
-template <> struct PT<float> {
+__device__ __forceinline__ float ex2neg(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(-x));
+  return y;
+}
+
+// Value-type traits: V = F2 (two FP32 targets per lane group) or double (one FP64 target).
+template <typename V> struct VT;
+template <> struct VT<F2> {
+  using Scalar = float;
+  static constexpr int kLanes = 2;
   // sqrt(log2(e) / 2): exp(-r^2/(2 sigma^2)) == 2^-(s r)^2 with s = kScale / sigma.
   static constexpr double kScale = 0.84932180028801904272;
   using Partial = float2;  // (hi, lo) of the compensated chunk sum
-  static __device__ __forceinline__ float expneg(float r2) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(-r2));
-    return y;
+  static __device__ __forceinline__ F2 zero() { return f2(0.f, 0.f); }
+  static __device__ __forceinline__ F2 dup(double a) { return f2((float)a, (float)a); }
+  static __device__ __forceinline__ F2 pack(double a, double b) { return f2((float)a, (float)b); }
+  static __device__ __forceinline__ F2 expneg(F2 r2) {
+    float a, b;
+    split(r2, a, b);
+    return f2(ex2neg(a), ex2neg(b));
+  }
+  static __device__ __forceinline__ double lane(F2 v, int k) {
+    float a, b;
+    split(v, a, b);
+    return k ? (double)b : (double)a;
   }
 };
-
-template <> struct PT<double> {
+template <> struct VT<double> {
+  using Scalar = double;
+  static constexpr int kLanes = 1;
   static constexpr double kScale = 0.70710678118654752440;  // sqrt(1/2): exp(-(s r)^2)
   using Partial = double;
+  static __device__ __forceinline__ double zero() { return 0.0; }
+  static __device__ __forceinline__ double dup(double a) { return a; }
+  static __device__ __forceinline__ double pack(double a, double) { return a; }
   static __device__ __forceinline__ double expneg(double r2) { return exp(-r2); }
+  static __device__ __forceinline__ double lane(double v, int) { return v; }
 };
 
-// Compensated accumulator: a tile sum `t` (plain FP32) is folded into (hi, lo) by Knuth's two-sum.
-template <typename R> struct Comp;
-template <> struct Comp<float> {
-  float hi, lo;
-  __device__ __forceinline__ void zero() { hi = 0.f; lo = 0.f; }
-  __device__ __forceinline__ void merge(float t) {
-    float s = __fadd_rn(hi, t);
-    float bp = __fsub_rn(s, hi);
-    float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(t, bp));
+// Compensated accumulator: a tile sum `t` is folded into (hi, lo) by Knuth's two-sum (FP32); plain sum (FP64).
+template <typename V> struct Comp;
+template <> struct Comp<F2> {
+  F2 hi, lo;
+  __device__ __forceinline__ void zero() { hi = lo = f2(0.f, 0.f); }
+  __device__ __forceinline__ void merge(F2 t) {
+    const F2 s = hi + t;
+    const F2 bp = s - hi;
+    const F2 err = (hi - (s - bp)) + (t - bp);
     hi = s;
-    lo = __fadd_rn(lo, err);
+    lo = lo + err;
   }
-  __device__ __forceinline__ float2 partial() const { return make_float2(hi, lo); }
+  __device__ __forceinline__ float2 partial(int k) const {
+    return make_float2((float)VT<F2>::lane(hi, k), (float)VT<F2>::lane(lo, k));
+  }
 };
 template <> struct Comp<double> {
   double hi;
   __device__ __forceinline__ void zero() { hi = 0.0; }
   __device__ __forceinline__ void merge(double t) { hi += t; }
-  __device__ __forceinline__ double partial() const { return hi; }
+  __device__ __forceinline__ double partial(int) const { return hi; }
 };
 
 __device__ __forceinline__ double partial_value(float2 p) { return (double)p.x + (double)p.y; }
 __device__ __forceinline__ double partial_value(double p) { return p; }
+
+__device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
 
 // Geometry shared by every op: centred, pre-scaled coordinates.
 struct Frame {
@@ -88,18 +149,21 @@ struct Frame {
   double inv_s2;      // 1 / sigma^2
 };
 
-template <typename R>
-__device__ __forceinline__ void load_point(const double* __restrict__ p, int i, const Frame& f, R& a, R& b, R& c) {
-  a = (R)((p[3 * i + 0] - f.o0) * f.s);
-  b = (R)((p[3 * i + 1] - f.o1) * f.s);
-  c = (R)((p[3 * i + 2] - f.o2) * f.s);
-}
+// Shared-memory unit: two source fields (each a duplicated FP32 pair or one FP64 value), 16 bytes.
+template <typename V>
+struct alignas(16) Unit {
+  V a, b;
+};
 
-template <typename R>
-__device__ __forceinline__ void load_vec(const double* __restrict__ p, int i, R& a, R& b, R& c) {
-  a = (R)p[3 * i + 0];
-  b = (R)p[3 * i + 1];
-  c = (R)p[3 * i + 2];
+// Per-target loaders: field values of targets i0, i1 packed into one V (V = double ignores i1).
+template <typename V>
+__device__ __forceinline__ V tgt_coord(const double* __restrict__ p, int i0, int i1, int c, double o, double s) {
+  return VT<V>::pack((p[3 * i0 + c] - o) * s, (p[3 * i1 + c] - o) * s);
+}
+template <typename V>
+__device__ __forceinline__ V tgt_field(const double* __restrict__ p, int stride, int i0, int i1, int c,
+                                       double scale = 1.0) {
+  return VT<V>::pack(scale * p[(size_t)stride * i0 + c], scale * p[(size_t)stride * i1 + c]);
 }
 
 // Launch plan of one all-pairs sum: gx target blocks x S source chunks of `chunk` sources (multiple of TPB).
@@ -110,21 +174,18 @@ struct Plan {
 
 int device_sm_count();
 
+// S is chosen so that gx * S CTAs fit in one wave of `ctas_per_sm` resident CTAs per SM (no tail wave); large
+// problems (gx >= one wave) use S = 1.
 template <int TPB, int RT>
 inline Plan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ctas_per_sm) {
   Plan p;
   if (n <= 0) return p;
   const int64_t tpb_targets = (int64_t)TPB * RT;
   p.gx = (int)((n + tpb_targets - 1) / tpb_targets);
-  if (m <= 0) {
-    p.S = 0;
-    p.chunk = 0;
-    p.ws_bytes = 0;
-    return p;
-  }
+  if (m <= 0) return p;
   const int64_t tiles = (m + TPB - 1) / TPB;
-  const int64_t want = (int64_t)device_sm_count() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
-  int64_t S = (want + p.gx - 1) / p.gx;
+  const int64_t wave = (int64_t)device_sm_count() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
+  int64_t S = wave / p.gx;
   if (S < 1) S = 1;
   if (S > tiles) S = tiles;
   const int64_t tiles_per_chunk = (tiles + S - 1) / S;
@@ -136,29 +197,36 @@ inline Plan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ct
 
 // ---------------------------------------------------------------------------------------------------------
 // Generic tiled all-pairs kernel.
-//   Op::NV        number of V4<R> records per source staged in shared memory
-//   Op::NA        number of scalar accumulators per target
-//   Op::Tgt       per-target register state
-//   Op::load_target(P, i, tgt)            (i < n)
-//   Op::load_source(P, l, V4<R>* rec)     (l < m)
-//   Op::pair(tgt, const V4<R>* src, R* acc)
+//   Op::NS         number of source fields (scalars) staged per source (NU = ceil(NS/2) 16-byte units)
+//   Op::NA         number of accumulators per target
+//   Op::template Tgt<V>                                  per-lane-group register state
+//   Op::template load_target<V>(P, i0, i1, tgt)          (i0, i1 < n; i1 ignored for V = double)
+//   Op::source_fields(P, l, double* f)                   the NS source fields of source l (l < m), FP64
+//   Op::template pair<V>(tgt, const V* s, V* acc)
 // Output: ws[(chunk * NA + c) * n + i] = compensated partial of accumulator c of target i.
 // ---------------------------------------------------------------------------------------------------------
-template <class Op, typename R, int TPB, int RT>
+template <class Op, typename V, int TPB, int RT>
 __global__ void __launch_bounds__(TPB) pairs_kernel(const typename Op::Params P, int n, int m, int chunk,
-                                                    typename PT<R>::Partial* __restrict__ ws) {
-  __shared__ V4<R> sm[Op::NV][TPB];
-  typename Op::Tgt tgt[RT];
-  R acc[RT][Op::NA];
-  Comp<R> cmp[RT][Op::NA];
+                                                    typename VT<V>::Partial* __restrict__ ws) {
+  constexpr int L = VT<V>::kLanes;
+  constexpr int G = RT / L;  // lane groups per thread
+  constexpr int NU = (Op::NS + 1) / 2;
+  static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
+  __shared__ Unit<V> sm[NU][TPB];
+  typename Op::template Tgt<V> tgt[G];
+  V acc[G][Op::NA];
+  Comp<V> cmp[G][Op::NA];
 
+  // target of (group g, lane k): base + (g * L + k) * TPB
   const int base = blockIdx.x * (TPB * RT) + threadIdx.x;
 #pragma unroll
-  for (int r = 0; r < RT; ++r) {
-    const int i = base + r * TPB;
-    Op::load_target(P, i < n ? i : (n - 1), tgt[r]);
+  for (int g = 0; g < G; ++g) {
+    int i0 = base + (g * L) * TPB, i1 = base + (g * L + L - 1) * TPB;
+    i0 = i0 < n ? i0 : n - 1;
+    i1 = i1 < n ? i1 : n - 1;
+    Op::template load_target<V>(P, i0, i1, tgt[g]);
 #pragma unroll
-    for (int c = 0; c < Op::NA; ++c) cmp[r][c].zero();
+    for (int c = 0; c < Op::NA; ++c) cmp[g][c].zero();
   }
 
   const int l_begin = blockIdx.y * chunk;
@@ -167,49 +235,60 @@ __global__ void __launch_bounds__(TPB) pairs_kernel(const typename Op::Params P,
 
   for (int l0 = l_begin; l0 < l_end; l0 += TPB) {
     const int l = l0 + threadIdx.x;
-    if (l < l_end) {
-      V4<R> rec[Op::NV];
-      Op::load_source(P, l, rec);
+    {
+      double f[2 * NU];
 #pragma unroll
-      for (int v = 0; v < Op::NV; ++v) sm[v][threadIdx.x] = rec[v];
-    } else {
+      for (int u = 0; u < 2 * NU; ++u) f[u] = 0.0;
+      if (l < l_end) Op::source_fields(P, l, f);
 #pragma unroll
-      for (int v = 0; v < Op::NV; ++v) sm[v][threadIdx.x] = V4<R>{R(0), R(0), R(0), R(0)};
+      for (int u = 0; u < NU; ++u) {
+        Unit<V> w;
+        w.a = VT<V>::dup(f[2 * u]);
+        w.b = VT<V>::dup(f[2 * u + 1]);
+        sm[u][threadIdx.x] = w;
+      }
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < RT; ++r)
+    for (int g = 0; g < G; ++g)
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) acc[r][c] = R(0);
+      for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<V>::zero();
 #pragma unroll 4
     for (int j = 0; j < TPB; ++j) {
-      V4<R> src[Op::NV];
+      V s[2 * NU];
 #pragma unroll
-      for (int v = 0; v < Op::NV; ++v) src[v] = sm[v][j];
+      for (int u = 0; u < NU; ++u) {
+        const Unit<V> w = sm[u][j];
+        s[2 * u] = w.a;
+        s[2 * u + 1] = w.b;
+      }
 #pragma unroll
-      for (int r = 0; r < RT; ++r) Op::pair(tgt[r], src, acc[r]);
+      for (int g = 0; g < G; ++g) Op::template pair<V>(tgt[g], s, acc[g]);
     }
 #pragma unroll
-    for (int r = 0; r < RT; ++r)
+    for (int g = 0; g < G; ++g)
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) cmp[r][c].merge(acc[r][c]);
+      for (int c = 0; c < Op::NA; ++c) cmp[g][c].merge(acc[g][c]);
     __syncthreads();
   }
 
 #pragma unroll
-  for (int r = 0; r < RT; ++r) {
-    const int i = base + r * TPB;
-    if (i < n) {
+  for (int g = 0; g < G; ++g)
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) ws[((size_t)blockIdx.y * Op::NA + c) * (size_t)n + i] = cmp[r][c].partial();
+    for (int k = 0; k < L; ++k) {
+      const int i = base + (g * L + k) * TPB;
+      if (i < n) {
+#pragma unroll
+        for (int c = 0; c < Op::NA; ++c)
+          ws[((size_t)blockIdx.y * Op::NA + c) * (size_t)n + i] = cmp[g][c].partial(k);
+      }
     }
-  }
 }
 
 // Epilogue: reduce the S chunk partials of target i in FP64 (fixed order) and hand them to Op::finalize.
-template <class Op, typename R>
+template <class Op, typename V>
 __global__ void finalize_kernel(const typename Op::Params P, int n, int S,
-                                const typename PT<R>::Partial* __restrict__ ws) {
+                                const typename VT<V>::Partial* __restrict__ ws) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double acc[Op::NA];
@@ -224,27 +303,39 @@ __global__ void finalize_kernel(const typename Op::Params P, int n, int S,
 // Deterministic single-block sum of `count` doubles: out[0] = (accumulate ? out[0] : 0) + scale * sum(v).
 __global__ void ordered_sum_kernel(const double* __restrict__ v, int count, double scale, double* out, int accumulate);
 
-template <class Op, typename R, int TPB, int RT>
+int resident_ctas(const void* kernel, int threads);
+
+template <class Op, typename V, int TPB, int RT>
+inline int ctas_per_sm() {
+  static int cached = 0;
+  if (cached == 0) {
+    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel<Op, V, TPB, RT>), TPB);
+    cached = c > 0 ? c : 4;
+  }
+  return cached;
+}
+
+template <class Op, typename V, int TPB, int RT>
 inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* ws, size_t ws_bytes,
-                     cudaStream_t stream, int ctas_per_sm) {
+                     cudaStream_t stream) {
   if (n <= 0) return kOk;
   if (n > INT32_MAX / 4 || m > INT32_MAX / 4) return kInvalidArgument;
-  Plan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename PT<R>::Partial), ctas_per_sm);
+  Plan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT>());
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (plan.ws_bytes > 0 && ws == nullptr) return kInvalidArgument;
-  auto* part = reinterpret_cast<typename PT<R>::Partial*>(ws);
+  auto* part = reinterpret_cast<typename VT<V>::Partial*>(ws);
   if (plan.S > 0) {
     dim3 grid(plan.gx, plan.S);
-    pairs_kernel<Op, R, TPB, RT><<<grid, TPB, 0, stream>>>(P, (int)n, (int)m, plan.chunk, part);
+    pairs_kernel<Op, V, TPB, RT><<<grid, TPB, 0, stream>>>(P, (int)n, (int)m, plan.chunk, part);
   }
   const int fb = 256;
-  finalize_kernel<Op, R><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.S, part);
+  finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.S, part);
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
-template <class Op, typename R, int TPB, int RT>
-inline size_t pairs_ws_bytes(int64_t n, int64_t m, int ctas_per_sm) {
-  return make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename PT<R>::Partial), ctas_per_sm).ws_bytes;
+template <class Op, typename V, int TPB, int RT>
+inline size_t pairs_ws_bytes(int64_t n, int64_t m) {
+  return make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT>()).ws_bytes;
 }
 
 inline Frame make_frame(const double* origin, double sigma, double kscale) {
@@ -259,5 +350,12 @@ inline Frame make_frame(const double* origin, double sigma, double kscale) {
 }
 
 inline bool bad_sigma(double sigma) { return !(sigma > 0.0) || !(sigma < 1e300); }
+
+// Source point in the frame (FP64 before the per-path conversion).
+__device__ __forceinline__ void src_point(const double* __restrict__ p, int l, const Frame& f, double* o) {
+  o[0] = (p[3 * l + 0] - f.o0) * f.s;
+  o[1] = (p[3 * l + 1] - f.o1) * f.s;
+  o[2] = (p[3 * l + 2] - f.o2) * f.s;
+}
 
 }  // namespace lddmm

@@ -9,35 +9,39 @@ namespace lddmm {
 // Second-order forward step (secondOrderEvolution loop body, base/pointEvolution.py:433-449):
 //   x1 = x + dt K(x) a,   a1 = a + dt za with za = -DK^T(x; a, a) = kappa sum_l e (a_k.a_l) d.
 // Accumulators: X = sum e a_l (3), A = sum e (a_k.a_l) d (3). 16 FP32 + 1 SFU per pair.
-template <typename R>
 struct OpSOFwd {
-  static constexpr int NV = 2, NA = 6;
+  static constexpr int NS = 6, NA = 6;
   struct Params {
     const double *x, *a;
     double *x1, *a1;
     Frame f;
     double dt;
   };
-  struct Tgt { R y0, y1, y2, a0, a1, a2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.x, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.a, i, t.a0, t.a1, t.a2);
+  template <typename V> struct Tgt { V y0, y1, y2, a0, a1, a2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.a0 = tgt_field<V>(P.a, 3, i0, i1, 0);
+    t.a1 = tgt_field<V>(P.a, 3, i0, i1, 1);
+    t.a2 = tgt_field<V>(P.a, 3, i0, i1, 2);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
-    s[0].w = s[1].w = R(0);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
+    f[3] = P.a[3 * l]; f[4] = P.a[3 * l + 1]; f[5] = P.a[3 * l + 2];
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    acc[0] += e * s[1].x;
-    acc[1] += e * s[1].y;
-    acc[2] += e * s[1].z;
-    const R ec = e * (t.a0 * s[1].x + t.a1 * s[1].y + t.a2 * s[1].z);
-    acc[3] += ec * d0;
-    acc[4] += ec * d1;
-    acc[5] += ec * d2;
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    acc[0] = fma(e, s[3], acc[0]);
+    acc[1] = fma(e, s[4], acc[1]);
+    acc[2] = fma(e, s[5], acc[2]);
+    const V ec = e * dot3(t.a0, t.a1, t.a2, s[3], s[4], s[5]);
+    acc[3] = fma(ec, d0, acc[3]);
+    acc[4] = fma(ec, d1, acc[4]);
+    acc[5] = fma(ec, d2, acc[5]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double ka = P.dt * P.f.kappa;
@@ -51,64 +55,72 @@ struct OpSOFwd {
 // Second-order adjoint step (secondOrderCovector loop body, base/pointEvolution.py:539-546):
 //   zpx = DK^T_sym(x; px, a) - DDK11and12(x; a, a, pa),   zpa = K(x) px - DK1and2(x; pa, a)
 //   px_prev = px + dt zpx,  pa_prev = pa + dt zpa.
-// With c1' = px'_k.a_l + a_k.px'_l (px' = -kappa px), c2'' = a''_k.a_l (a'' = -kappa^2 a), q = dpa = pa_k - pa_l,
-// dq = d.q the accumulators are
+// With c1' = px'_k.a_l + a_k.px'_l (px' = -kappa px), c2'' = a''_k.a_l (a'' = -kappa^2 a), dq = d.(pa_k - pa_l)
+// the accumulators are
 //   G = sum e (c1' + c2'' dq) d (3), C = sum e c2'' (1), D = sum e c2'' pa_l (3), E = sum e px'_l (3),
 //   F = sum e dq a_l (3)
 // and zpx = G + (pa_k C - D)/(sigma^2 (-kappa^2)), zpa = E/(-kappa) + kappa F. 38 FP32 + 1 SFU per pair.
-template <typename R>
 struct OpSOBwd {
-  static constexpr int NV = 3, NA = 13;
+  static constexpr int NS = 12, NA = 13;
   struct Params {
     const double *x, *a, *px, *pa;
     double *px_prev, *pa_prev;
     Frame f;
     double dt;
   };
-  struct Tgt { R y0, y1, y2, a0, a1, a2, b0, b1, b2, p0, p1, p2, q0, q1, q2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
+  template <typename V> struct Tgt { V y0, y1, y2, a0, a1, a2, b0, b1, b2, p0, p1, p2, q0, q1, q2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
     const double k = P.f.kappa;
-    load_point(P.x, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.a, i, t.a0, t.a1, t.a2);
-    t.b0 = (R)(-k * k * P.a[3 * i + 0]);
-    t.b1 = (R)(-k * k * P.a[3 * i + 1]);
-    t.b2 = (R)(-k * k * P.a[3 * i + 2]);
-    t.p0 = (R)(-k * P.px[3 * i + 0]);
-    t.p1 = (R)(-k * P.px[3 * i + 1]);
-    t.p2 = (R)(-k * P.px[3 * i + 2]);
-    load_vec(P.pa, i, t.q0, t.q1, t.q2);
+    t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.a0 = tgt_field<V>(P.a, 3, i0, i1, 0);
+    t.a1 = tgt_field<V>(P.a, 3, i0, i1, 1);
+    t.a2 = tgt_field<V>(P.a, 3, i0, i1, 2);
+    t.b0 = tgt_field<V>(P.a, 3, i0, i1, 0, -k * k);
+    t.b1 = tgt_field<V>(P.a, 3, i0, i1, 1, -k * k);
+    t.b2 = tgt_field<V>(P.a, 3, i0, i1, 2, -k * k);
+    t.p0 = tgt_field<V>(P.px, 3, i0, i1, 0, -k);
+    t.p1 = tgt_field<V>(P.px, 3, i0, i1, 1, -k);
+    t.p2 = tgt_field<V>(P.px, 3, i0, i1, 2, -k);
+    t.q0 = tgt_field<V>(P.pa, 3, i0, i1, 0);
+    t.q1 = tgt_field<V>(P.pa, 3, i0, i1, 1);
+    t.q2 = tgt_field<V>(P.pa, 3, i0, i1, 2);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
+  // fields: x' (0-2), a (3-5), pa (6-8), px' = -kappa px (9-11)
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
     const double k = P.f.kappa;
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
-    load_vec(P.pa, l, s[2].x, s[2].y, s[2].z);
-    s[0].w = (R)(-k * P.px[3 * l + 0]);
-    s[1].w = (R)(-k * P.px[3 * l + 1]);
-    s[2].w = (R)(-k * P.px[3 * l + 2]);
+    src_point(P.x, l, P.f, f);
+    for (int c = 0; c < 3; ++c) {
+      f[3 + c] = P.a[3 * l + c];
+      f[6 + c] = P.pa[3 * l + c];
+      f[9 + c] = -k * P.px[3 * l + c];
+    }
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    const R dq = d0 * (t.q0 - s[2].x) + d1 * (t.q1 - s[2].y) + d2 * (t.q2 - s[2].z);
-    const R c1 = t.p0 * s[1].x + t.p1 * s[1].y + t.p2 * s[1].z + t.a0 * s[0].w + t.a1 * s[1].w + t.a2 * s[2].w;
-    const R c2 = t.b0 * s[1].x + t.b1 * s[1].y + t.b2 * s[1].z;
-    const R eg = e * (c1 + c2 * dq);
-    acc[0] += eg * d0;
-    acc[1] += eg * d1;
-    acc[2] += eg * d2;
-    const R ec2 = e * c2;
-    acc[3] += ec2;
-    acc[4] += ec2 * s[2].x;
-    acc[5] += ec2 * s[2].y;
-    acc[6] += ec2 * s[2].z;
-    acc[7] += e * s[0].w;
-    acc[8] += e * s[1].w;
-    acc[9] += e * s[2].w;
-    const R edq = e * dq;
-    acc[10] += edq * s[1].x;
-    acc[11] += edq * s[1].y;
-    acc[12] += edq * s[1].z;
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V dq = dot3(d0, d1, d2, t.q0 - s[6], t.q1 - s[7], t.q2 - s[8]);
+    const V c1 = fma(t.a2, s[11], fma(t.a1, s[10], fma(t.a0, s[9], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
+    const V c2 = dot3(t.b0, t.b1, t.b2, s[3], s[4], s[5]);
+    const V eg = e * fma(c2, dq, c1);
+    acc[0] = fma(eg, d0, acc[0]);
+    acc[1] = fma(eg, d1, acc[1]);
+    acc[2] = fma(eg, d2, acc[2]);
+    const V ec2 = e * c2;
+    acc[3] = acc[3] + ec2;
+    acc[4] = fma(ec2, s[6], acc[4]);
+    acc[5] = fma(ec2, s[7], acc[5]);
+    acc[6] = fma(ec2, s[8], acc[6]);
+    acc[7] = fma(e, s[9], acc[7]);
+    acc[8] = fma(e, s[10], acc[8]);
+    acc[9] = fma(e, s[11], acc[9]);
+    const V edq = e * dq;
+    acc[10] = fma(edq, s[3], acc[10]);
+    acc[11] = fma(edq, s[4], acc[11]);
+    acc[12] = fma(edq, s[5], acc[12]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = P.f.kappa;
@@ -128,9 +140,8 @@ struct OpSOBwd {
 //   p_t = p_{t+1} + dt DK^T_lddmm(x_t; p_{t+1}, a_t) = p_{t+1} - dt kappa sum_l e (p_k.a_l + a_k.q_l) d,
 //   q_l = p_l - 2 w a_l;  dat_t = K(x_t)(2 w a_t - p_{t+1}) = -sum_l e q_l (euclidean) or 2 w a_t - p_{t+1}.
 // Accumulators: A = sum e c d (3), Q = sum e q_l (3). 19 FP32 + 1 SFU per pair.
-template <typename R>
 struct OpFOBwd {
-  static constexpr int NV = 3, NA = 6;
+  static constexpr int NS = 9, NA = 6;
   struct Params {
     const double *x, *a, *p;
     double *p_prev, *dat;
@@ -138,32 +149,38 @@ struct OpFOBwd {
     double dt, w;
     int euclidean;
   };
-  struct Tgt { R y0, y1, y2, p0, p1, p2, a0, a1, a2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    load_point(P.x, i, P.f, t.y0, t.y1, t.y2);
-    load_vec(P.p, i, t.p0, t.p1, t.p2);
-    load_vec(P.a, i, t.a0, t.a1, t.a2);
+  template <typename V> struct Tgt { V y0, y1, y2, p0, p1, p2, a0, a1, a2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.p0 = tgt_field<V>(P.p, 3, i0, i1, 0);
+    t.p1 = tgt_field<V>(P.p, 3, i0, i1, 1);
+    t.p2 = tgt_field<V>(P.p, 3, i0, i1, 2);
+    t.a0 = tgt_field<V>(P.a, 3, i0, i1, 0);
+    t.a1 = tgt_field<V>(P.a, 3, i0, i1, 1);
+    t.a2 = tgt_field<V>(P.a, 3, i0, i1, 2);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_point(P.x, l, P.f, s[0].x, s[0].y, s[0].z);
-    load_vec(P.a, l, s[1].x, s[1].y, s[1].z);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    src_point(P.x, l, P.f, f);
     for (int c = 0; c < 3; ++c) {
-      const R q = (R)(P.p[3 * l + c] - 2.0 * P.w * P.a[3 * l + c]);
-      if (c == 0) s[2].x = q; else if (c == 1) s[2].y = q; else s[2].z = q;
+      f[3 + c] = P.a[3 * l + c];
+      f[6 + c] = P.p[3 * l + c] - 2.0 * P.w * P.a[3 * l + c];
     }
-    s[0].w = s[1].w = s[2].w = R(0);
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
-    const R c = t.p0 * s[1].x + t.p1 * s[1].y + t.p2 * s[1].z + t.a0 * s[2].x + t.a1 * s[2].y + t.a2 * s[2].z;
-    const R ec = e * c;
-    acc[0] += ec * d0;
-    acc[1] += ec * d1;
-    acc[2] += ec * d2;
-    acc[3] += e * s[2].x;
-    acc[4] += e * s[2].y;
-    acc[5] += e * s[2].z;
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V c = fma(t.a2, s[8], fma(t.a1, s[7], fma(t.a0, s[6], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
+    const V ec = e * c;
+    acc[0] = fma(ec, d0, acc[0]);
+    acc[1] = fma(ec, d1, acc[1]);
+    acc[2] = fma(ec, d2, acc[2]);
+    acc[3] = fma(e, s[6], acc[3]);
+    acc[4] = fma(e, s[7], acc[4]);
+    acc[5] = fma(e, s[8], acc[5]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = P.dt * P.f.kappa;
@@ -179,39 +196,57 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
   size_t b = 0;
   auto upd = [&](size_t v) { b = v > b ? v : b; };
   if (precision == kFP32Compensated) {
-    upd(pairs_ws_bytes<OpSOFwd<float>, float, kTpbLight, kRtLight>(n, n, kCtasPerSm));
-    upd(pairs_ws_bytes<OpSOBwd<float>, float, kTpbHeavy, kRtHeavy>(n, n, kCtasPerSm));
-    upd(pairs_ws_bytes<OpFOBwd<float>, float, kTpbLight, kRtLight>(n, n, kCtasPerSm));
-    upd(pairs_ws_bytes<OpK<float>, float, kTpbLight, kRtLight>(n, n, kCtasPerSm));
+    upd(pairs_ws_bytes<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
+    upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtHeavy>(n, n));
+    upd(pairs_ws_bytes<OpFOBwd, F2, kTpbLight, kRtLight>(n, n));
+    upd(pairs_ws_bytes<OpK, F2, kTpbLight, kRtLight>(n, n));
   } else {
-    upd(pairs_ws_bytes<OpSOBwd<double>, double, kTpb64, kRt64>(n, n, kCtasPerSm));
-    upd(pairs_ws_bytes<OpK<double>, double, kTpb64, kRt64>(n, n, kCtasPerSm));
+    upd(pairs_ws_bytes<OpSOFwd, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes<OpSOBwd, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes<OpFOBwd, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes<OpK, double, kTpb64, kRt64>(n, n));
   }
   // per-point dot products for the FP64 energy reductions live after the pair partials
-  return b + (size_t)(n > 0 ? n : 0) * sizeof(double) + 256;
+  return ((b + 255) & ~(size_t)255) + (size_t)(n > 0 ? n : 0) * sizeof(double);
 }
 
 namespace {
+
+// Launch shapes per precision: light (forward / first-order) and heavy (second-order adjoint) ops.
+template <typename V> struct Shape;
+template <> struct Shape<F2> {
+  static constexpr int kTpb = kTpbLight, kRt = kRtLight, kTpbH = kTpbHeavy, kRtH = kRtHeavy;
+};
+template <> struct Shape<double> {
+  static constexpr int kTpb = kTpb64, kRt = kRt64, kTpbH = kTpb64, kRtH = kRt64;
+};
+
+template <typename V>
+inline Frame frame(const double* origin, double sigma) {
+  return make_frame(origin, sigma, VT<V>::kScale);
+}
 
 inline double* dots_region(void* ws, size_t pair_bytes) {
   size_t off = (pair_bytes + 255) & ~(size_t)255;
   return reinterpret_cast<double*>(reinterpret_cast<char*>(ws) + off);
 }
 
-template <typename R, int TPB, int RT>
+// out = base_sign * base + scale * K(x) a, and (energy != NULL) energy = [acc ? energy : 0] + escale * sum_i dotw_i.(K a)_i
+template <typename V>
 int k_energy_and_update(const double* x, const double* a, int64_t n, const Frame& f, const double* base,
                         double base_sign, double scale, double* out, const double* dotw, double* energy,
                         double escale, int accumulate, void* ws, size_t wsb, cudaStream_t st) {
-  typename OpK<R>::Params P;
+  constexpr int TPB = Shape<V>::kTpb, RT = Shape<V>::kRt;
+  OpK::Params P;
   P.y = x; P.x = x; P.a = a; P.out = out; P.f = f;
   P.base = base; P.base_sign = base_sign; P.scale = scale;
-  const size_t pb = pairs_ws_bytes<OpK<R>, R, TPB, RT>(n, n, kCtasPerSm);
+  const size_t pb = pairs_ws_bytes<OpK, V, TPB, RT>(n, n);
   if (energy) {
     if (((pb + 255) & ~(size_t)255) + (size_t)n * sizeof(double) > wsb) return kWorkspaceTooSmall;
     P.dotw = dotw;
     P.dots = dots_region(ws, pb);
   }
-  int rc = run_pairs<OpK<R>, R, TPB, RT>(P, n, n, ws, wsb, st, kCtasPerSm);
+  int rc = run_pairs<OpK, V, TPB, RT>(P, n, n, ws, wsb, st);
   if (rc != kOk) return rc;
   if (energy) {
     ordered_sum_kernel<<<1, 1024, 0, st>>>(P.dots, (int)n, escale, energy, accumulate);
@@ -220,24 +255,35 @@ int k_energy_and_update(const double* x, const double* a, int64_t n, const Frame
   return kOk;
 }
 
-template <typename R, int TPB, int RT, int TPBH, int RTH>
+template <typename V>
+int so_step(const double* x, const double* a, int64_t n, const Frame& f, double dt, double* x1, double* a1, void* ws,
+            size_t wsb, cudaStream_t st) {
+  OpSOFwd::Params P{x, a, x1, a1, f, dt};
+  return run_pairs<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
+}
+
+template <typename V>
+int so_adjoint_step(const double* x, const double* a, const double* px, const double* pa, int64_t n, const Frame& f,
+                    double dt, double* px_prev, double* pa_prev, void* ws, size_t wsb, cudaStream_t st) {
+  OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt};
+  return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH>(P, n, n, ws, wsb, st);
+}
+
+template <typename V>
 int so_shoot(const double* x0, const double* a0, int64_t n, int64_t T, const Frame& f, double dt, double* xt,
              double* at, void* ws, size_t wsb, cudaStream_t st) {
   const size_t stride = (size_t)n * 3;
   if (cudaMemcpyAsync(xt, x0, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return kCudaError;
   if (cudaMemcpyAsync(at, a0, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return kCudaError;
   for (int64_t t = 0; t < T; ++t) {
-    typename OpSOFwd<R>::Params P;
-    P.x = xt + t * stride; P.a = at + t * stride;
-    P.x1 = xt + (t + 1) * stride; P.a1 = at + (t + 1) * stride;
-    P.f = f; P.dt = dt;
-    int rc = run_pairs<OpSOFwd<R>, R, TPB, RT>(P, n, n, ws, wsb, st, kCtasPerSm);
+    int rc = so_step<V>(xt + t * stride, at + t * stride, n, f, dt, xt + (t + 1) * stride, at + (t + 1) * stride, ws,
+                        wsb, st);
     if (rc != kOk) return rc;
   }
   return kOk;
 }
 
-template <typename R, int TPB, int RT, int TPBH, int RTH>
+template <typename V>
 int so_gradient(const double* xt, const double* at, int64_t n, int64_t T, const Frame& f, double dt,
                 const double* px1, const double* pa1, double* pxt, double* pat, double* da0, void* ws, size_t wsb,
                 cudaStream_t st) {
@@ -247,16 +293,46 @@ int so_gradient(const double* xt, const double* at, int64_t n, int64_t T, const 
   if (cudaMemcpyAsync(pat + T * stride, pa1, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
     return kCudaError;
   for (int64_t t = T - 1; t >= 0; --t) {
-    typename OpSOBwd<R>::Params P;
-    P.x = xt + t * stride; P.a = at + t * stride;
-    P.px = pxt + (t + 1) * stride; P.pa = pat + (t + 1) * stride;
-    P.px_prev = pxt + t * stride; P.pa_prev = pat + t * stride;
-    P.f = f; P.dt = dt;
-    int rc = run_pairs<OpSOBwd<R>, R, TPBH, RTH>(P, n, n, ws, wsb, st, kCtasPerSm);
+    int rc = so_adjoint_step<V>(xt + t * stride, at + t * stride, pxt + (t + 1) * stride, pat + (t + 1) * stride, n, f,
+                                dt, pxt + t * stride, pat + t * stride, ws, wsb, st);
     if (rc != kOk) return rc;
   }
-  if (da0)
-    return k_energy_and_update<R, TPB, RT>(xt, at, n, f, pat, -1.0, 1.0, da0, nullptr, nullptr, 0.0, 0, ws, wsb, st);
+  if (da0) return k_energy_and_update<V>(xt, at, n, f, pat, -1.0, 1.0, da0, nullptr, nullptr, 0.0, 0, ws, wsb, st);
+  return kOk;
+}
+
+template <typename V>
+int fo_shoot(const double* x0, const double* at, int64_t n, int64_t T, const Frame& f, double regweight, double* xt,
+             double* energy, void* ws, size_t wsb, cudaStream_t st) {
+  const size_t stride = (size_t)n * 3;
+  if (cudaMemcpyAsync(xt, x0, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return kCudaError;
+  if (T == 0 && energy) {
+    if (cudaMemsetAsync(energy, 0, sizeof(double), st) != cudaSuccess) return kCudaError;
+  }
+  const double dt = T > 0 ? 1.0 / (double)T : 0.0;
+  for (int64_t t = 0; t < T; ++t) {
+    const double* x = xt + t * stride;
+    const double* a = at + t * stride;
+    int rc = k_energy_and_update<V>(x, a, n, f, x, 1.0, dt, xt + (t + 1) * stride, a, energy, regweight * dt, t > 0,
+                                    ws, wsb, st);
+    if (rc != kOk) return rc;
+  }
+  return kOk;
+}
+
+template <typename V>
+int fo_gradient(const double* xt, const double* at, int64_t n, int64_t T, const Frame& f, double regweight,
+                const double* px1, int euclidean, double* pxt, double* dat, void* ws, size_t wsb, cudaStream_t st) {
+  const size_t stride = (size_t)n * 3;
+  if (cudaMemcpyAsync(pxt + T * stride, px1, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return kCudaError;
+  const double dt = T > 0 ? 1.0 / (double)T : 0.0;
+  for (int64_t t = T - 1; t >= 0; --t) {
+    OpFOBwd::Params P{xt + t * stride, at + t * stride, pxt + (t + 1) * stride, pxt + t * stride, dat + t * stride,
+                      f, dt, regweight, euclidean};
+    int rc = run_pairs<OpFOBwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
+    if (rc != kOk) return rc;
+  }
   return kOk;
 }
 
@@ -267,6 +343,9 @@ bool bad(const void* p, int64_t n) { return n > 0 && p == nullptr; }
 
 using namespace lddmm;
 
+#define LDDMM_DISPATCH(precision, call_f2, call_f64) \
+  ((precision) == kFP32Compensated ? (call_f2) : ((precision) == kFP64 ? (call_f64) : (int)kInvalidArgument))
+
 extern "C" {
 
 int lddmm_second_order_step(const double* x, const double* a, int64_t n, double sigma, double dt,
@@ -274,15 +353,8 @@ int lddmm_second_order_step(const double* x, const double* a, int64_t n, double 
                             size_t wsb, lddmm_stream_t stream) {
   if (n < 0 || bad_sigma(sigma) || bad(x, n) || bad(a, n) || bad(x_next, n) || bad(a_next, n)) return kInvalidArgument;
   cudaStream_t st = (cudaStream_t)stream;
-  if (precision == kFP32Compensated) {
-    OpSOFwd<float>::Params P{x, a, x_next, a_next, make_frame(origin, sigma, PT<float>::kScale), dt};
-    return run_pairs<OpSOFwd<float>, float, kTpbLight, kRtLight>(P, n, n, ws, wsb, st, kCtasPerSm);
-  }
-  if (precision == kFP64) {
-    OpSOFwd<double>::Params P{x, a, x_next, a_next, make_frame(origin, sigma, PT<double>::kScale), dt};
-    return run_pairs<OpSOFwd<double>, double, kTpb64, kRt64>(P, n, n, ws, wsb, st, kCtasPerSm);
-  }
-  return kInvalidArgument;
+  return LDDMM_DISPATCH(precision, so_step<F2>(x, a, n, frame<F2>(origin, sigma), dt, x_next, a_next, ws, wsb, st),
+                        so_step<double>(x, a, n, frame<double>(origin, sigma), dt, x_next, a_next, ws, wsb, st));
 }
 
 int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int64_t T, double sigma, double dt,
@@ -291,13 +363,8 @@ int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int6
   if (n < 0 || T < 0 || bad_sigma(sigma) || bad(x0, n) || bad(a0, n) || bad(xt, n) || bad(at, n)) return kInvalidArgument;
   if (n == 0) return kOk;
   cudaStream_t st = (cudaStream_t)stream;
-  if (precision == kFP32Compensated)
-    return so_shoot<float, kTpbLight, kRtLight, kTpbHeavy, kRtHeavy>(
-        x0, a0, n, T, make_frame(origin, sigma, PT<float>::kScale), dt, xt, at, ws, wsb, st);
-  if (precision == kFP64)
-    return so_shoot<double, kTpb64, kRt64, kTpb64, kRt64>(x0, a0, n, T, make_frame(origin, sigma, PT<double>::kScale),
-                                                          dt, xt, at, ws, wsb, st);
-  return kInvalidArgument;
+  return LDDMM_DISPATCH(precision, so_shoot<F2>(x0, a0, n, T, frame<F2>(origin, sigma), dt, xt, at, ws, wsb, st),
+                        so_shoot<double>(x0, a0, n, T, frame<double>(origin, sigma), dt, xt, at, ws, wsb, st));
 }
 
 int lddmm_second_order_adjoint_step(const double* x, const double* a, const double* px, const double* pa, int64_t n,
@@ -307,15 +374,9 @@ int lddmm_second_order_adjoint_step(const double* x, const double* a, const doub
       bad(pa_prev, n))
     return kInvalidArgument;
   cudaStream_t st = (cudaStream_t)stream;
-  if (precision == kFP32Compensated) {
-    OpSOBwd<float>::Params P{x, a, px, pa, px_prev, pa_prev, make_frame(origin, sigma, PT<float>::kScale), dt};
-    return run_pairs<OpSOBwd<float>, float, kTpbHeavy, kRtHeavy>(P, n, n, ws, wsb, st, kCtasPerSm);
-  }
-  if (precision == kFP64) {
-    OpSOBwd<double>::Params P{x, a, px, pa, px_prev, pa_prev, make_frame(origin, sigma, PT<double>::kScale), dt};
-    return run_pairs<OpSOBwd<double>, double, kTpb64, kRt64>(P, n, n, ws, wsb, st, kCtasPerSm);
-  }
-  return kInvalidArgument;
+  return LDDMM_DISPATCH(
+      precision, so_adjoint_step<F2>(x, a, px, pa, n, frame<F2>(origin, sigma), dt, px_prev, pa_prev, ws, wsb, st),
+      so_adjoint_step<double>(x, a, px, pa, n, frame<double>(origin, sigma), dt, px_prev, pa_prev, ws, wsb, st));
 }
 
 int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, double dt,
@@ -326,44 +387,20 @@ int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, i
     return kInvalidArgument;
   if (n == 0) return kOk;
   cudaStream_t st = (cudaStream_t)stream;
-  if (precision == kFP32Compensated)
-    return so_gradient<float, kTpbLight, kRtLight, kTpbHeavy, kRtHeavy>(
-        xt, at, n, T, make_frame(origin, sigma, PT<float>::kScale), dt, px1, pa1, pxt, pat, da0, ws, wsb, st);
-  if (precision == kFP64)
-    return so_gradient<double, kTpb64, kRt64, kTpb64, kRt64>(
-        xt, at, n, T, make_frame(origin, sigma, PT<double>::kScale), dt, px1, pa1, pxt, pat, da0, ws, wsb, st);
-  return kInvalidArgument;
+  return LDDMM_DISPATCH(
+      precision, so_gradient<F2>(xt, at, n, T, frame<F2>(origin, sigma), dt, px1, pa1, pxt, pat, da0, ws, wsb, st),
+      so_gradient<double>(xt, at, n, T, frame<double>(origin, sigma), dt, px1, pa1, pxt, pat, da0, ws, wsb, st));
 }
 
 int lddmm_first_order_shoot(const double* x0, const double* at, int64_t n, int64_t T, double sigma, double regweight,
                             const double* origin, double* xt, double* energy, int precision, void* ws, size_t wsb,
                             lddmm_stream_t stream) {
   if (n < 0 || T < 0 || bad_sigma(sigma) || bad(x0, n) || bad(at, n) || bad(xt, n)) return kInvalidArgument;
-  cudaStream_t st = (cudaStream_t)stream;
-  const size_t stride = (size_t)n * 3;
   if (n == 0) return kOk;
-  if (cudaMemcpyAsync(xt, x0, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return kCudaError;
-  if (T == 0 && energy) {
-    if (cudaMemsetAsync(energy, 0, sizeof(double), st) != cudaSuccess) return kCudaError;
-  }
-  const double dt = T > 0 ? 1.0 / (double)T : 0.0;
-  for (int64_t t = 0; t < T; ++t) {
-    const double* x = xt + t * stride;
-    const double* a = at + t * stride;
-    int rc;
-    if (precision == kFP32Compensated)
-      rc = k_energy_and_update<float, kTpbLight, kRtLight>(x, a, n, make_frame(origin, sigma, PT<float>::kScale), x,
-                                                           1.0, dt, xt + (t + 1) * stride, a, energy,
-                                                           regweight * dt, t > 0, ws, wsb, st);
-    else if (precision == kFP64)
-      rc = k_energy_and_update<double, kTpb64, kRt64>(x, a, n, make_frame(origin, sigma, PT<double>::kScale), x, 1.0,
-                                                      dt, xt + (t + 1) * stride, a, energy, regweight * dt, t > 0, ws,
-                                                      wsb, st);
-    else
-      return kInvalidArgument;
-    if (rc != kOk) return rc;
-  }
-  return kOk;
+  cudaStream_t st = (cudaStream_t)stream;
+  return LDDMM_DISPATCH(
+      precision, fo_shoot<F2>(x0, at, n, T, frame<F2>(origin, sigma), regweight, xt, energy, ws, wsb, st),
+      fo_shoot<double>(x0, at, n, T, frame<double>(origin, sigma), regweight, xt, energy, ws, wsb, st));
 }
 
 int lddmm_first_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma,
@@ -373,28 +410,11 @@ int lddmm_first_order_gradient(const double* xt, const double* at, int64_t n, in
     return kInvalidArgument;
   if (n == 0) return kOk;
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t stride = (size_t)n * 3;
-  if (cudaMemcpyAsync(pxt + T * stride, px1, stride * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return kCudaError;
-  const double dt = T > 0 ? 1.0 / (double)T : 0.0;
-  for (int64_t t = T - 1; t >= 0; --t) {
-    int rc;
-    if (precision == kFP32Compensated) {
-      OpFOBwd<float>::Params P{xt + t * stride, at + t * stride, pxt + (t + 1) * stride, pxt + t * stride,
-                               dat + t * stride, make_frame(origin, sigma, PT<float>::kScale), dt, regweight,
-                               euclidean};
-      rc = run_pairs<OpFOBwd<float>, float, kTpbLight, kRtLight>(P, n, n, ws, wsb, st, kCtasPerSm);
-    } else if (precision == kFP64) {
-      OpFOBwd<double>::Params P{xt + t * stride, at + t * stride, pxt + (t + 1) * stride, pxt + t * stride,
-                                dat + t * stride, make_frame(origin, sigma, PT<double>::kScale), dt, regweight,
-                                euclidean};
-      rc = run_pairs<OpFOBwd<double>, double, kTpb64, kRt64>(P, n, n, ws, wsb, st, kCtasPerSm);
-    } else {
-      return kInvalidArgument;
-    }
-    if (rc != kOk) return rc;
-  }
-  return kOk;
+  return LDDMM_DISPATCH(
+      precision,
+      fo_gradient<F2>(xt, at, n, T, frame<F2>(origin, sigma), regweight, px1, euclidean, pxt, dat, ws, wsb, st),
+      fo_gradient<double>(xt, at, n, T, frame<double>(origin, sigma), regweight, px1, euclidean, pxt, dat, ws, wsb,
+                          st));
 }
 
 }  // extern "C"

@@ -57,64 +57,75 @@ __device__ __forceinline__ const FaceRec& src_face(const FaceSources& S, int l, 
   return S.B[l - S.mA];
 }
 
-template <typename R>
-__device__ __forceinline__ void face_point(const FaceRec& r, const Frame& f, R& a, R& b, R& c) {
-  a = (R)((r.c[0] - f.o0) * f.s);
-  b = (R)((r.c[1] - f.o1) * f.s);
-  c = (R)((r.c[2] - f.o2) * f.s);
-}
-
-// Source record: (c', aw * factor) and the unit normal, or (c') and the weighted surfel * factor (current).
-template <typename R, int KIND>
-__device__ __forceinline__ void load_face_source(const FaceSources& S, const Frame& f, int l, V4<R>* s) {
+// Source fields: centre' (0-2), aw * factor (3), unit normal (4-6); current: centre', 0, fw * surfel * factor.
+template <int KIND>
+__device__ __forceinline__ void face_source_fields(const FaceSources& S, const Frame& f, int l, double* o) {
   double fac;
   const FaceRec& r = src_face(S, l, fac);
-  face_point(r, f, s[0].x, s[0].y, s[0].z);
+  o[0] = (r.c[0] - f.o0) * f.s;
+  o[1] = (r.c[1] - f.o1) * f.s;
+  o[2] = (r.c[2] - f.o2) * f.s;
   if (KIND == LDDMM_DATA_CURRENT) {
-    s[0].w = R(0);
-    s[1].x = (R)(fac * r.s[0] * r.fw);
-    s[1].y = (R)(fac * r.s[1] * r.fw);
-    s[1].z = (R)(fac * r.s[2] * r.fw);
+    o[3] = 0.0;
+    for (int c = 0; c < 3; ++c) o[4 + c] = fac * r.s[c] * r.fw;
   } else {
-    s[0].w = (R)(fac * r.aw);
-    s[1].x = (R)r.n[0];
-    s[1].y = (R)r.n[1];
-    s[1].z = (R)r.n[2];
+    o[3] = fac * r.aw;
+    for (int c = 0; c < 3; ++c) o[4 + c] = r.n[c];
   }
-  s[1].w = R(0);
 }
 
-// ---- energies: dots[k] = weight_k * sum_l e_kl payload_kl ----
-template <typename R, int KIND>
+// Target lane-group state: centre' and the unit normal (varifold, measure) or fw * surfel (current).
+template <typename V> struct FaceTgt { V y0, y1, y2, n0, n1, n2; };
+
+template <typename V, int KIND>
+__device__ __forceinline__ void load_face_target(const FaceRec* T, const Frame& f, int i0, int i1, FaceTgt<V>& t) {
+  const FaceRec &r0 = T[i0], &r1 = T[i1];
+  t.y0 = VT<V>::pack((r0.c[0] - f.o0) * f.s, (r1.c[0] - f.o0) * f.s);
+  t.y1 = VT<V>::pack((r0.c[1] - f.o1) * f.s, (r1.c[1] - f.o1) * f.s);
+  t.y2 = VT<V>::pack((r0.c[2] - f.o2) * f.s, (r1.c[2] - f.o2) * f.s);
+  if (KIND == LDDMM_DATA_CURRENT) {
+    t.n0 = VT<V>::pack(r0.s[0] * r0.fw, r1.s[0] * r1.fw);
+    t.n1 = VT<V>::pack(r0.s[1] * r0.fw, r1.s[1] * r1.fw);
+    t.n2 = VT<V>::pack(r0.s[2] * r0.fw, r1.s[2] * r1.fw);
+  } else {
+    t.n0 = VT<V>::pack(r0.n[0], r1.n[0]);
+    t.n1 = VT<V>::pack(r0.n[1], r1.n[1]);
+    t.n2 = VT<V>::pack(r0.n[2], r1.n[2]);
+  }
+}
+
+// ---- energies: dots[k] = weight_k * sum_l e_kl payload_kl. Varifold 13 FP32 + 1 SFU per pair. ----
+template <int KIND>
 struct OpSurfEnergy {
-  static constexpr int NV = 2, NA = (KIND == LDDMM_DATA_CURRENT) ? 3 : 1;
+  static constexpr int NS = 7, NA = (KIND == LDDMM_DATA_CURRENT) ? 3 : 1;
   struct Params {
     const FaceRec* T;
     FaceSources S;
     double* dots;
     Frame f;
   };
-  struct Tgt { R y0, y1, y2, n0, n1, n2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    const FaceRec& r = P.T[i];
-    face_point(r, P.f, t.y0, t.y1, t.y2);
-    t.n0 = (R)r.n[0]; t.n1 = (R)r.n[1]; t.n2 = (R)r.n[2];
+  template <typename V> using Tgt = FaceTgt<V>;
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    load_face_target<V, KIND>(P.T, P.f, i0, i1, t);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_face_source<R, KIND>(P.S, P.f, l, s);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    face_source_fields<KIND>(P.S, P.f, l, f);
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
     if (KIND == LDDMM_DATA_VARIFOLD) {
-      const R g = t.n0 * s[1].x + t.n1 * s[1].y + t.n2 * s[1].z;
-      acc[0] += (e * s[0].w) * (R(1) + g * g);
+      const V g = dot3(t.n0, t.n1, t.n2, s[4], s[5], s[6]);
+      const V ea = e * s[3];
+      acc[0] = fma(ea, g * g, acc[0] + ea);
     } else if (KIND == LDDMM_DATA_MEASURE) {
-      acc[0] += e * s[0].w;
+      acc[0] = fma(e, s[3], acc[0]);
     } else {
-      acc[0] += e * s[1].x;
-      acc[1] += e * s[1].y;
-      acc[2] += e * s[1].z;
+      acc[0] = fma(e, s[4], acc[0]);
+      acc[1] = fma(e, s[5], acc[1]);
+      acc[2] = fma(e, s[6], acc[2]);
     }
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
@@ -131,60 +142,58 @@ struct FaceGrad {
   double z[3], dz[3], zw, pad;
 };
 
-template <typename R, int KIND>
+// Varifold gradient pair: z += e aw_l [2g n_l + (1-g^2) n_k] (as Z = sum 2g e aw n_l and W = sum e aw (1-g^2)),
+// D = sum e aw (1+g^2) d, S = sum e aw (1+g^2): 22 FP32 + 1 SFU per pair.
+template <int KIND>
 struct OpSurfGrad {
-  static constexpr int NV = 2, NA = (KIND == LDDMM_DATA_VARIFOLD) ? 8 : (KIND == LDDMM_DATA_CURRENT ? 6 : 4);
+  static constexpr int NS = 7, NA = (KIND == LDDMM_DATA_VARIFOLD) ? 8 : (KIND == LDDMM_DATA_CURRENT ? 6 : 4);
   struct Params {
     const FaceRec* T;
     FaceSources S;
     FaceGrad* out;
     Frame f;
   };
-  struct Tgt { R y0, y1, y2, n0, n1, n2; };
-  static __device__ __forceinline__ void load_target(const Params& P, int i, Tgt& t) {
-    const FaceRec& r = P.T[i];
-    face_point(r, P.f, t.y0, t.y1, t.y2);
-    if (KIND == LDDMM_DATA_CURRENT) {
-      t.n0 = (R)(r.s[0] * r.fw); t.n1 = (R)(r.s[1] * r.fw); t.n2 = (R)(r.s[2] * r.fw);
-    } else {
-      t.n0 = (R)r.n[0]; t.n1 = (R)r.n[1]; t.n2 = (R)r.n[2];
-    }
+  template <typename V> using Tgt = FaceTgt<V>;
+  template <typename V>
+  static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    load_face_target<V, KIND>(P.T, P.f, i0, i1, t);
   }
-  static __device__ __forceinline__ void load_source(const Params& P, int l, V4<R>* s) {
-    load_face_source<R, KIND>(P.S, P.f, l, s);
+  static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
+    face_source_fields<KIND>(P.S, P.f, l, f);
   }
-  static __device__ __forceinline__ void pair(const Tgt& t, const V4<R>* s, R* acc) {
-    const R d0 = t.y0 - s[0].x, d1 = t.y1 - s[0].y, d2 = t.y2 - s[0].z;
-    const R e = PT<R>::expneg(d0 * d0 + d1 * d1 + d2 * d2);
+  template <typename V>
+  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+    const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
     if (KIND == LDDMM_DATA_VARIFOLD) {
-      // z: sum e aw_l [2g n_l + (1-g^2) n_k]; d: sum e aw_l (1+g^2) d; sw: sum e aw_l (1+g^2)
-      const R g = t.n0 * s[1].x + t.n1 * s[1].y + t.n2 * s[1].z;
-      const R ea = e * s[0].w;
-      const R f = R(1) + g * g;
-      const R t2 = R(2) * g * ea;
-      acc[0] += t2 * s[1].x;
-      acc[1] += t2 * s[1].y;
-      acc[2] += t2 * s[1].z;
-      acc[3] += ea * (R(1) - g * g);
-      const R eaf = ea * f;
-      acc[4] += eaf * d0;
-      acc[5] += eaf * d1;
-      acc[6] += eaf * d2;
-      acc[7] += eaf;
+      const V g = dot3(t.n0, t.n1, t.n2, s[4], s[5], s[6]);
+      const V ea = e * s[3];
+      const V eag = ea * g;
+      const V eag2 = eag * g;
+      const V t2 = eag + eag;
+      acc[0] = fma(t2, s[4], acc[0]);
+      acc[1] = fma(t2, s[5], acc[1]);
+      acc[2] = fma(t2, s[6], acc[2]);
+      acc[3] = acc[3] + (ea - eag2);
+      const V eaf = ea + eag2;
+      acc[4] = fma(eaf, d0, acc[4]);
+      acc[5] = fma(eaf, d1, acc[5]);
+      acc[6] = fma(eaf, d2, acc[6]);
+      acc[7] = acc[7] + eaf;
     } else if (KIND == LDDMM_DATA_CURRENT) {
-      acc[0] += e * s[1].x;
-      acc[1] += e * s[1].y;
-      acc[2] += e * s[1].z;
-      const R ec = e * (t.n0 * s[1].x + t.n1 * s[1].y + t.n2 * s[1].z);
-      acc[3] += ec * d0;
-      acc[4] += ec * d1;
-      acc[5] += ec * d2;
+      acc[0] = fma(e, s[4], acc[0]);
+      acc[1] = fma(e, s[5], acc[1]);
+      acc[2] = fma(e, s[6], acc[2]);
+      const V ec = e * dot3(t.n0, t.n1, t.n2, s[4], s[5], s[6]);
+      acc[3] = fma(ec, d0, acc[3]);
+      acc[4] = fma(ec, d1, acc[4]);
+      acc[5] = fma(ec, d2, acc[5]);
     } else {
-      const R ea = e * s[0].w;
-      acc[0] += ea;
-      acc[1] += ea * d0;
-      acc[2] += ea * d1;
-      acc[3] += ea * d2;
+      const V ea = e * s[3];
+      acc[0] = acc[0] + ea;
+      acc[1] = fma(ea, d0, acc[1]);
+      acc[2] = fma(ea, d1, acc[2]);
+      acc[3] = fma(ea, d2, acc[3]);
     }
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
@@ -252,14 +261,19 @@ struct SurfLayout {
   size_t recs, grads, dots, pairs, total;
 };
 
-template <typename R, int TPB, int RT>
+template <typename V, int TPB, int RT>
 size_t surf_pairs_bytes(int64_t nf, int64_t nf1) {
   size_t b = 0;
   auto upd = [&](size_t v) { b = v > b ? v : b; };
-  upd(pairs_ws_bytes<OpSurfGrad<R, LDDMM_DATA_VARIFOLD>, R, TPB, RT>(nf, nf + nf1, kCtasPerSm));
-  upd(pairs_ws_bytes<OpSurfEnergy<R, LDDMM_DATA_CURRENT>, R, TPB, RT>(nf, nf + nf1, kCtasPerSm));
-  upd(pairs_ws_bytes<OpSurfEnergy<R, LDDMM_DATA_CURRENT>, R, TPB, RT>(nf1, nf1, kCtasPerSm));
-  upd(pairs_ws_bytes<OpSurfGrad<R, LDDMM_DATA_CURRENT>, R, TPB, RT>(nf, nf + nf1, kCtasPerSm));
+  upd(pairs_ws_bytes<OpSurfGrad<LDDMM_DATA_VARIFOLD>, V, TPB, RT>(nf, nf + nf1));
+  upd(pairs_ws_bytes<OpSurfGrad<LDDMM_DATA_CURRENT>, V, TPB, RT>(nf, nf + nf1));
+  upd(pairs_ws_bytes<OpSurfGrad<LDDMM_DATA_MEASURE>, V, TPB, RT>(nf, nf + nf1));
+  for (int64_t n : {nf, nf1}) {
+    const int64_t m = (n == nf) ? nf + nf1 : nf1;
+    upd(pairs_ws_bytes<OpSurfEnergy<LDDMM_DATA_VARIFOLD>, V, TPB, RT>(n, m));
+    upd(pairs_ws_bytes<OpSurfEnergy<LDDMM_DATA_CURRENT>, V, TPB, RT>(n, m));
+    upd(pairs_ws_bytes<OpSurfEnergy<LDDMM_DATA_MEASURE>, V, TPB, RT>(n, m));
+  }
   return b;
 }
 
@@ -269,25 +283,25 @@ SurfLayout surf_layout(int64_t nf, int64_t nf1, int precision) {
   L.grads = L.recs + align256(sizeof(FaceRec) * (size_t)(nf + nf1));
   L.dots = L.grads + align256(sizeof(FaceGrad) * (size_t)nf);
   L.pairs = L.dots + align256(sizeof(double) * (size_t)(nf > nf1 ? nf : nf1));
-  const size_t pb = precision == kFP32Compensated ? surf_pairs_bytes<float, kTpbLight, kRtLight>(nf, nf1)
+  const size_t pb = precision == kFP32Compensated ? surf_pairs_bytes<F2, kTpbLight, kRtLight>(nf, nf1)
                                                   : surf_pairs_bytes<double, kTpb64, kRt64>(nf, nf1);
   L.total = L.pairs + align256(pb);
   return L;
 }
 
-template <typename R, int TPB, int RT, int KIND>
+template <typename V, int TPB, int RT, int KIND>
 int surf_energy(const FaceRec* def, int nf, const FaceRec* tgt, int nf1, const Frame& f, int with_norm0,
                 double* energy, double* dots, void* pairs, size_t pairs_bytes, cudaStream_t st) {
-  using Op = OpSurfEnergy<R, KIND>;
+  using Op = OpSurfEnergy<KIND>;
   typename Op::Params P;
   P.T = def; P.S = FaceSources{def, nf, tgt, -2.0}; P.dots = dots; P.f = f;
-  int rc = run_pairs<Op, R, TPB, RT>(P, nf, (int64_t)nf + nf1, pairs, pairs_bytes, st, kCtasPerSm);
+  int rc = run_pairs<Op, V, TPB, RT>(P, nf, (int64_t)nf + nf1, pairs, pairs_bytes, st);
   if (rc != kOk) return rc;
   if (nf > 0) ordered_sum_kernel<<<1, 1024, 0, st>>>(dots, nf, 1.0, energy, 0);
   else if (cudaMemsetAsync(energy, 0, sizeof(double), st) != cudaSuccess) return kCudaError;
   if (with_norm0) {
     P.T = tgt; P.S = FaceSources{tgt, nf1, nullptr, 0.0};
-    rc = run_pairs<Op, R, TPB, RT>(P, nf1, nf1, pairs, pairs_bytes, st, kCtasPerSm);
+    rc = run_pairs<Op, V, TPB, RT>(P, nf1, nf1, pairs, pairs_bytes, st);
     if (rc != kOk) return rc;
     if (nf1 > 0) ordered_sum_kernel<<<1, 1024, 0, st>>>(dots, nf1, 1.0, energy + 1, 0);
     else if (cudaMemsetAsync(energy + 1, 0, sizeof(double), st) != cudaSuccess) return kCudaError;
@@ -295,13 +309,13 @@ int surf_energy(const FaceRec* def, int nf, const FaceRec* tgt, int nf1, const F
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
-template <typename R, int TPB, int RT, int KIND>
+template <typename V, int TPB, int RT, int KIND>
 int surf_grad(const FaceRec* def, int nf, const FaceRec* tgt, int nf1, const Frame& f, FaceGrad* grads, void* pairs,
               size_t pairs_bytes, cudaStream_t st) {
-  using Op = OpSurfGrad<R, KIND>;
+  using Op = OpSurfGrad<KIND>;
   typename Op::Params P;
   P.T = def; P.S = FaceSources{def, nf, tgt, -1.0}; P.out = grads; P.f = f;
-  return run_pairs<Op, R, TPB, RT>(P, nf, (int64_t)nf + nf1, pairs, pairs_bytes, st, kCtasPerSm);
+  return run_pairs<Op, V, TPB, RT>(P, nf, (int64_t)nf + nf1, pairs, pairs_bytes, st);
 }
 
 template <int KIND>
@@ -309,9 +323,9 @@ int surf_energy_dispatch(int precision, const FaceRec* def, int nf, const FaceRe
                          double sigma, int with_norm0, double* energy, double* dots, void* pairs, size_t pb,
                          cudaStream_t st) {
   if (precision == kFP32Compensated)
-    return surf_energy<float, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, PT<float>::kScale),
-                                                         with_norm0, energy, dots, pairs, pb, st);
-  return surf_energy<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, PT<double>::kScale),
+    return surf_energy<F2, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<F2>::kScale),
+                                                      with_norm0, energy, dots, pairs, pb, st);
+  return surf_energy<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<double>::kScale),
                                                   with_norm0, energy, dots, pairs, pb, st);
 }
 
@@ -319,9 +333,9 @@ template <int KIND>
 int surf_grad_dispatch(int precision, const FaceRec* def, int nf, const FaceRec* tgt, int nf1, const double* origin,
                        double sigma, FaceGrad* grads, void* pairs, size_t pb, cudaStream_t st) {
   if (precision == kFP32Compensated)
-    return surf_grad<float, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, PT<float>::kScale),
-                                                       grads, pairs, pb, st);
-  return surf_grad<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, PT<double>::kScale),
+    return surf_grad<F2, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<F2>::kScale),
+                                                    grads, pairs, pb, st);
+  return surf_grad<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<double>::kScale),
                                                 grads, pairs, pb, st);
 }
 
