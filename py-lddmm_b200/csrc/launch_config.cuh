@@ -1,18 +1,36 @@
-// Launch shapes of the all-pairs kernels (threads per CTA x targets per thread), chosen for 148 SMs.
+// Launch shapes of the all-pairs kernels (threads per CTA x targets per thread). The defaults were chosen by
+// timing on the B200; each can be overridden at build time (-DLDDMM_RT_LIGHT=... etc.) for tuning sweeps.
 #pragma once
+
+#ifndef LDDMM_TPB_LIGHT
+#define LDDMM_TPB_LIGHT 128
+#endif
+#ifndef LDDMM_RT_LIGHT
+#define LDDMM_RT_LIGHT 4
+#endif
+#ifndef LDDMM_TPB_HEAVY
+#define LDDMM_TPB_HEAVY 128
+#endif
+#ifndef LDDMM_RT_HEAVY
+#define LDDMM_RT_HEAVY 2
+#endif
+#ifndef LDDMM_TPB_64
+#define LDDMM_TPB_64 128
+#endif
+#ifndef LDDMM_RT_64
+#define LDDMM_RT_64 2
+#endif
 
 namespace lddmm {
 
-// Light ops (<= 6 accumulators per target): 4 targets per thread amortise each broadcast LDS over 4 pairs.
-constexpr int kTpbLight = 128;
-constexpr int kRtLight = 4;
-// Heavy ops (7-16 accumulators per target): 2 targets per thread keeps registers under 128.
-constexpr int kTpbHeavy = 128;
-constexpr int kRtHeavy = 2;
+// Light ops (<= 8 accumulators per target): several targets per thread amortise each broadcast LDS.
+constexpr int kTpbLight = LDDMM_TPB_LIGHT;
+constexpr int kRtLight = LDDMM_RT_LIGHT;
+// Heavy ops (the 13-accumulator second-order adjoint, the 7-accumulator DDK): fewer targets per thread.
+constexpr int kTpbHeavy = LDDMM_TPB_HEAVY;
+constexpr int kRtHeavy = LDDMM_RT_HEAVY;
 // FP64 baseline path.
-constexpr int kTpb64 = 128;
-constexpr int kRt64 = 2;
-// Source-chunk split: aim for this many resident CTAs per SM when the target blocks alone are too few.
-constexpr int kCtasPerSm = 4;
+constexpr int kTpb64 = LDDMM_TPB_64;
+constexpr int kRt64 = LDDMM_RT_64;
 
 }  // namespace lddmm

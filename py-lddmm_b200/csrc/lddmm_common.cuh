@@ -3,9 +3,10 @@
 // Every hot operator of the point-set path is a map-reduce over (target k, source l) pairs:
 //     out_k = epilogue_k( sum_l pair(target_k, source_l) ).
 // The pair loop is FP32-pipe / MUFU bound (arithmetic intensity >> 100 flop/byte), so the design is an N-body
-// tiling: a CTA owns TPB*RT targets held in registers (RT per thread), streams tiles of TPB sources through
-// shared memory (all threads of a warp read the same source record: broadcast LDS.128), and the source range is
-// split into S chunks along gridDim.y so that mid-size problems fill all 148 SMs.
+// tiling: a CTA owns TPB*RT targets held in registers (RT per thread) and streams tiles of TPB sources through
+// shared memory (all threads of a warp read the same source record: broadcast LDS.128). The (target block, source
+// tile) units are split evenly over exactly one resident wave of CTAs (stream-K style, see SKPlan), so every
+// problem size keeps all 148 SMs equally busy.
 //
 // FP32 path: the pair arithmetic runs on Blackwell's packed FP32 instructions (fma/add/sub/mul .f32x2): one
 // instruction evaluates the same source against TWO targets of the thread, halving the issue slots of the FP32
@@ -166,31 +167,49 @@ __device__ __forceinline__ V tgt_field(const double* __restrict__ p, int stride,
   return VT<V>::pack(scale * p[(size_t)stride * i0 + c], scale * p[(size_t)stride * i1 + c]);
 }
 
-// Launch plan of one all-pairs sum: gx target blocks x S source chunks of `chunk` sources (multiple of TPB).
-struct Plan {
-  int gx = 0, S = 0, chunk = 0;
+// ---------------------------------------------------------------------------------------------------------
+// Stream-K style launch plan. The work of one all-pairs sum is W = gx * TT units (gx target blocks of TPB*RT
+// targets, TT source tiles of TPB sources). C = min(W, one resident wave) CTAs each take the contiguous unit range
+// [start(c), start(c+1)), start(c) = floor(c W / C): every SM gets the same number of pair evaluations (to one
+// tile), whatever n and m are. A CTA walks its range as segments (one target block, a run of tiles) and writes
+// one compensated partial per segment; the partials of target block tb come from CTAs cta_of(tb TT) ..
+// cta_of((tb+1) TT - 1) and are stored in slot (c - cta_of(tb TT)), so the epilogue reduces them in a fixed order.
+// ---------------------------------------------------------------------------------------------------------
+struct SKPlan {
+  int gx = 0, TT = 0, C = 0, S = 0;  // S = max partial slots per target block
+  long long W = 0;
   size_t ws_bytes = 0;
 };
 
+__host__ __device__ __forceinline__ long long sk_start(long long c, long long W, long long C) { return c * W / C; }
+
+__host__ __device__ __forceinline__ int sk_cta_of(long long u, long long W, long long C) {
+  long long c = ((u + 1) * C - 1) / W;
+  while (c + 1 < C && sk_start(c + 1, W, C) <= u) ++c;
+  while (c > 0 && sk_start(c, W, C) > u) --c;
+  return (int)c;
+}
+
 int device_sm_count();
 
-// S is chosen so that gx * S CTAs fit in one wave of `ctas_per_sm` resident CTAs per SM (no tail wave); large
-// problems (gx >= one wave) use S = 1.
 template <int TPB, int RT>
-inline Plan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ctas_per_sm) {
-  Plan p;
+inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ctas_per_sm) {
+  SKPlan p;
   if (n <= 0) return p;
-  const int64_t tpb_targets = (int64_t)TPB * RT;
-  p.gx = (int)((n + tpb_targets - 1) / tpb_targets);
+  const int64_t tb_targets = (int64_t)TPB * RT;
+  p.gx = (int)((n + tb_targets - 1) / tb_targets);
   if (m <= 0) return p;
-  const int64_t tiles = (m + TPB - 1) / TPB;
-  const int64_t wave = (int64_t)device_sm_count() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
-  int64_t S = wave / p.gx;
-  if (S < 1) S = 1;
-  if (S > tiles) S = tiles;
-  const int64_t tiles_per_chunk = (tiles + S - 1) / S;
-  p.chunk = (int)(tiles_per_chunk * TPB);
-  p.S = (int)((m + p.chunk - 1) / p.chunk);
+  p.TT = (int)((m + TPB - 1) / TPB);
+  p.W = (long long)p.gx * p.TT;
+  const long long wave = (long long)device_sm_count() * (ctas_per_sm > 0 ? ctas_per_sm : 1);
+  p.C = (int)(p.W < wave ? p.W : wave);
+  int smax = 1;
+  for (int tb = 0; tb < p.gx; ++tb) {
+    const int c0 = sk_cta_of((long long)tb * p.TT, p.W, p.C);
+    const int c1 = sk_cta_of((long long)(tb + 1) * p.TT - 1, p.W, p.C);
+    if (c1 - c0 + 1 > smax) smax = c1 - c0 + 1;
+  }
+  p.S = smax;
   p.ws_bytes = (size_t)p.S * (size_t)na * (size_t)n * partial_bytes;
   return p;
 }
@@ -203,100 +222,110 @@ inline Plan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ct
 //   Op::template load_target<V>(P, i0, i1, tgt)          (i0, i1 < n; i1 ignored for V = double)
 //   Op::source_fields(P, l, double* f)                   the NS source fields of source l (l < m), FP64
 //   Op::template pair<V>(tgt, const V* s, V* acc)
-// Output: ws[(chunk * NA + c) * n + i] = compensated partial of accumulator c of target i.
+// Output: ws[(slot * NA + c) * n + i] = compensated partial of accumulator c of target i for one segment.
 // ---------------------------------------------------------------------------------------------------------
 template <class Op, typename V, int TPB, int RT>
-__global__ void __launch_bounds__(TPB) pairs_kernel(const typename Op::Params P, int n, int m, int chunk,
-                                                    typename VT<V>::Partial* __restrict__ ws) {
+__global__ void __launch_bounds__(TPB) pairs_kernel(const typename Op::Params P, int n, int m, int TT, long long W,
+                                                    int C, typename VT<V>::Partial* __restrict__ ws) {
   constexpr int L = VT<V>::kLanes;
   constexpr int G = RT / L;  // lane groups per thread
   constexpr int NU = (Op::NS + 1) / 2;
   static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
   __shared__ Unit<V> sm[NU][TPB];
-  typename Op::template Tgt<V> tgt[G];
-  V acc[G][Op::NA];
-  Comp<V> cmp[G][Op::NA];
 
-  // target of (group g, lane k): base + (g * L + k) * TPB
-  const int base = blockIdx.x * (TPB * RT) + threadIdx.x;
-#pragma unroll
-  for (int g = 0; g < G; ++g) {
-    int i0 = base + (g * L) * TPB, i1 = base + (g * L + L - 1) * TPB;
-    i0 = i0 < n ? i0 : n - 1;
-    i1 = i1 < n ? i1 : n - 1;
-    Op::template load_target<V>(P, i0, i1, tgt[g]);
-#pragma unroll
-    for (int c = 0; c < Op::NA; ++c) cmp[g][c].zero();
-  }
+  const long long u_end = sk_start(blockIdx.x + 1, W, C);
+  long long u = sk_start(blockIdx.x, W, C);
+  while (u < u_end) {
+    const int tb = (int)(u / TT);
+    const int j0 = (int)(u - (long long)tb * TT);
+    const int j1 = (int)((u_end - (long long)tb * TT) < TT ? (u_end - (long long)tb * TT) : TT);
+    const int slot = (int)blockIdx.x - sk_cta_of((long long)tb * TT, W, C);
 
-  const int l_begin = blockIdx.y * chunk;
-  int l_end = l_begin + chunk;
-  if (l_end > m) l_end = m;
-
-  for (int l0 = l_begin; l0 < l_end; l0 += TPB) {
-    const int l = l0 + threadIdx.x;
-    {
-      double f[2 * NU];
+    typename Op::template Tgt<V> tgt[G];
+    Comp<V> cmp[G][Op::NA];
+    // target of (group g, lane k): base + (g * L + k) * TPB
+    const int base = tb * (TPB * RT) + threadIdx.x;
 #pragma unroll
-      for (int u = 0; u < 2 * NU; ++u) f[u] = 0.0;
-      if (l < l_end) Op::source_fields(P, l, f);
+    for (int g = 0; g < G; ++g) {
+      int i0 = base + (g * L) * TPB, i1 = base + (g * L + L - 1) * TPB;
+      i0 = i0 < n ? i0 : n - 1;
+      i1 = i1 < n ? i1 : n - 1;
+      Op::template load_target<V>(P, i0, i1, tgt[g]);
 #pragma unroll
-      for (int u = 0; u < NU; ++u) {
-        Unit<V> w;
-        w.a = VT<V>::dup(f[2 * u]);
-        w.b = VT<V>::dup(f[2 * u + 1]);
-        sm[u][threadIdx.x] = w;
-      }
+      for (int c = 0; c < Op::NA; ++c) cmp[g][c].zero();
     }
-    __syncthreads();
+
+    for (int j = j0; j < j1; ++j) {
+      const int l = j * TPB + threadIdx.x;
+      {
+        double f[2 * NU];
 #pragma unroll
-    for (int g = 0; g < G; ++g)
+        for (int q = 0; q < 2 * NU; ++q) f[q] = 0.0;
+        if (l < m) Op::source_fields(P, l, f);
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<V>::zero();
+        for (int q = 0; q < NU; ++q) {
+          Unit<V> w;
+          w.a = VT<V>::dup(f[2 * q]);
+          w.b = VT<V>::dup(f[2 * q + 1]);
+          sm[q][threadIdx.x] = w;
+        }
+      }
+      __syncthreads();
+      V acc[G][Op::NA];
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<V>::zero();
 #pragma unroll 4
-    for (int j = 0; j < TPB; ++j) {
-      V s[2 * NU];
+      for (int jj = 0; jj < TPB; ++jj) {
+        V s[2 * NU];
 #pragma unroll
-      for (int u = 0; u < NU; ++u) {
-        const Unit<V> w = sm[u][j];
-        s[2 * u] = w.a;
-        s[2 * u + 1] = w.b;
+        for (int q = 0; q < NU; ++q) {
+          const Unit<V> w = sm[q][jj];
+          s[2 * q] = w.a;
+          s[2 * q + 1] = w.b;
+        }
+#pragma unroll
+        for (int g = 0; g < G; ++g) Op::template pair<V>(tgt[g], s, acc[g]);
       }
 #pragma unroll
-      for (int g = 0; g < G; ++g) Op::template pair<V>(tgt[g], s, acc[g]);
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int c = 0; c < Op::NA; ++c) cmp[g][c].merge(acc[g][c]);
+      __syncthreads();
     }
+
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) cmp[g][c].merge(acc[g][c]);
-    __syncthreads();
-  }
-
+      for (int k = 0; k < L; ++k) {
+        const int i = base + (g * L + k) * TPB;
+        if (i < n) {
 #pragma unroll
-  for (int g = 0; g < G; ++g)
-#pragma unroll
-    for (int k = 0; k < L; ++k) {
-      const int i = base + (g * L + k) * TPB;
-      if (i < n) {
-#pragma unroll
-        for (int c = 0; c < Op::NA; ++c)
-          ws[((size_t)blockIdx.y * Op::NA + c) * (size_t)n + i] = cmp[g][c].partial(k);
+          for (int c = 0; c < Op::NA; ++c)
+            ws[((size_t)slot * Op::NA + c) * (size_t)n + i] = cmp[g][c].partial(k);
+        }
       }
-    }
+    u += j1 - j0;
+  }
 }
 
-// Epilogue: reduce the S chunk partials of target i in FP64 (fixed order) and hand them to Op::finalize.
+// Epilogue: reduce the partial slots of target i (its block's CTAs, in CTA order) in FP64, then Op::finalize.
 template <class Op, typename V>
-__global__ void finalize_kernel(const typename Op::Params P, int n, int S,
+__global__ void finalize_kernel(const typename Op::Params P, int n, int tb_targets, int TT, long long W, int C,
                                 const typename VT<V>::Partial* __restrict__ ws) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double acc[Op::NA];
 #pragma unroll
   for (int c = 0; c < Op::NA; ++c) acc[c] = 0.0;
-  for (int s = 0; s < S; ++s)
+  if (W > 0) {
+    const int tb = i / tb_targets;
+    const int nslot = sk_cta_of((long long)(tb + 1) * TT - 1, W, C) - sk_cta_of((long long)tb * TT, W, C) + 1;
+    for (int s = 0; s < nslot; ++s)
 #pragma unroll
-    for (int c = 0; c < Op::NA; ++c) acc[c] += partial_value(ws[((size_t)s * Op::NA + c) * (size_t)n + i]);
+      for (int c = 0; c < Op::NA; ++c) acc[c] += partial_value(ws[((size_t)s * Op::NA + c) * (size_t)n + i]);
+  }
   Op::finalize(P, i, acc);
 }
 
@@ -320,16 +349,15 @@ inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* w
                      cudaStream_t stream) {
   if (n <= 0) return kOk;
   if (n > INT32_MAX / 4 || m > INT32_MAX / 4) return kInvalidArgument;
-  Plan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT>());
+  SKPlan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT>());
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (plan.ws_bytes > 0 && ws == nullptr) return kInvalidArgument;
   auto* part = reinterpret_cast<typename VT<V>::Partial*>(ws);
-  if (plan.S > 0) {
-    dim3 grid(plan.gx, plan.S);
-    pairs_kernel<Op, V, TPB, RT><<<grid, TPB, 0, stream>>>(P, (int)n, (int)m, plan.chunk, part);
-  }
+  if (plan.W > 0)
+    pairs_kernel<Op, V, TPB, RT><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C, part);
   const int fb = 256;
-  finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.S, part);
+  finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, TPB * RT, plan.TT, plan.W, plan.C,
+                                                                      part);
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
