@@ -84,6 +84,18 @@ int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m,
                          double* out, int precision, void* workspace, size_t workspace_bytes,
                          lddmm_stream_t stream);
 
+/* out(n,3) = K(y, x) a without any workspace argument and without allocating: lddmm_apply_k for callers that
+ * cannot allocate device memory at call time (an application whose device-memory budget is fixed at start-up, a
+ * plugin host that gives its plugins no allocator, or a latency-critical path that may not call cudaMalloc because
+ * it can synchronise the device). This entry point has no counterpart in the reference.
+ * Its scratch is a 32 MiB array built into the library; every GPU that loads the library holds it until exit.
+ * Limits: n <= 262,144 targets (any m); a request whose partial sums would not fit the array is rejected with
+ * LDDMM_ERR_WORKSPACE before any launch. The first call on a device looks up the array's address with that device
+ * current: make it before any stream capture. All calls share the array (nothing needs clearing between calls);
+ * calls that overlap on the GPU race on it and must be serialised by the caller. */
+int lddmm_apply_k_static(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
+                         const double* origin, double* out, int precision, lddmm_stream_t stream);
+
 /* Dense-weight variants (O(n m) weights streamed from HBM).
  * out(n,d) = sum_l K(y_k, x_l) u[k,l,:]  -- Kernel.applyK(matrixWeights=True) -> ku.applykmat  kernelFunctions_util.py:1509
  * out(n,3) = sum_l -(y_k-x_l)/sigma^2 K beta[k,l] -- Kernel.applyDiffKmat -> ku.applykdiffmat  kernelFunctions_util.py:1631 */

@@ -33,6 +33,7 @@ SIGNATURES = {
     'lddmm_apply_diff_k1and2': [_dp, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp, _sz, _vp],
     'lddmm_apply_divergence': [_dp, _i64, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp, _sz, _vp],
     'lddmm_apply_k_tensor': [_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _f64, _hp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_apply_k_static': [_dp, _i64, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp],
     'lddmm_apply_k_mat': [_dp, _i64, _dp, _i64, _dp, _i64, _f64, _dp, _vp],
     'lddmm_apply_diff_k_mat': [_dp, _i64, _dp, _i64, _dp, _f64, _dp, _vp],
     'lddmm_second_order_step': [_dp, _dp, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
