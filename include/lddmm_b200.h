@@ -185,6 +185,36 @@ int lddmm_surface_gradient(int kind, const double* xdef, int64_t nv, const int64
 int lddmm_vertex_face_table(const int64_t* faces_host, int64_t nf, int64_t nv, int32_t* vf_offsets_host,
                             int32_t* vf_items_host);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * Learned momentum proposal (north_star "learned part"; no counterpart in the reference, which has no learned
+ * component). Per-vertex MLP with BF16 weights / activations and FP32 accumulation on the tensor cores.
+ * ------------------------------------------------------------------------------------------------------- */
+
+/* C = epilogue(op(A) op(B)): A is (M,K) row-major, or stored transposed (K,M) when trans_a; B is (K,N) row-major, or
+ * stored transposed (N,K) when trans_b; bf16 operands, FP32 accumulation. M, N multiples of 64, K a multiple of 32.
+ * epilogue: 0 C f32 = acc (splits > 1 splits K over `splits` CTAs, reduced in fixed order through split_ws of
+ * splits*M*N floats); 1 C f32 = acc + bias; 2 C bf16 = relu(acc + bias); 3 C bf16 = acc + bias;
+ * 4 C bf16 = (mask > 0) ? acc : 0 with mask (M,N) bf16. */
+int lddmm_bf16_gemm(int trans_a, int trans_b, int epilogue, int64_t M, int64_t N, int64_t K, const void* A,
+                    const void* B, const float* bias, const void* mask, void* C, int splits, float* split_ws,
+                    size_t split_ws_bytes, lddmm_stream_t stream);
+
+/* db(N) = column sums of dy (M,N) bf16, FP32, fixed order. */
+int lddmm_bf16_colsum(const void* dy, int64_t M, int64_t N, float* db, lddmm_stream_t stream);
+
+/* Squared-error gradient of the first nout columns of y (M,N) f32 against target (M,nout) f32 for rows < valid:
+ * dy (M,N) bf16 = 2 w (y - target) there and 0 elsewhere; row_loss (M) f32 = per-row squared errors. */
+int lddmm_mse_grad(const float* y, int64_t M, int64_t N, const float* target, int64_t nout, int64_t valid, float w,
+                   void* dy, float* row_loss, lddmm_stream_t stream);
+
+/* Adam step on FP32 master weights (step >= 1, bias-corrected), writing the bf16 copy param_bf16 (may be NULL). */
+int lddmm_adam_step(float* param, const float* grad, float* m1, float* m2, void* param_bf16, int64_t count, float lr,
+                    float beta1, float beta2, float eps, int64_t step, float weight_decay, lddmm_stream_t stream);
+
+/* disp(n,3) = tgt[argmin_l |src_k - tgt_l|] - src_k: nearest-target displacement of every source point. */
+int lddmm_nearest_displacement(const double* src, int64_t n, const double* tgt, int64_t m, double* disp,
+                               lddmm_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,278 @@
+"""Learned initial-momentum proposal for geodesic surface matching (no counterpart in the reference).
+
+A per-vertex MLP maps local features of a (source, target) pair to the initial momentum a0 of
+SecondOrderSurfaceMatching; the plain optimiser then refines from that proposal and falls back to zero momentum
+when the proposal does not lower the objective (`warm_start`).
+
+Features per source vertex (all computed on the device by the library's kernels):
+  centred position (3), area-weighted vertex normal (3), nearest-target displacement d (3), its kernel-smoothed
+  versions sum_l K(x_k,x_l) d_l / sum_l K(x_k,x_l) at widths 0.25 and 0.5 (6, the kernel-smoothed aggregation over
+  the surface), normal component d.n (1), |d| (1) -> 17, zero-padded to 64 (the GEMM tile width).
+Network: 64 -> 128 -> 128 -> 128 -> 64 (outputs 0..2 used), ReLU, BF16 weights and activations, FP32 accumulation
+and FP32 master weights (Adam), all GEMMs in `lddmm_bf16_gemm` (mma.sync tensor cores).
+Output: the normal component (v0.n) n of the initial velocity v0 = K(x0) a0, over VELOCITY_SCALE. The velocity is a
+smooth, resolution-independent field (the raw momentum, a kernel inverse of it, is not), and only its normal part
+is determined by the target shape: tangential motion leaves the surface unchanged, is invisible to any shape
+feature and is left to the regulariser during refinement. The momentum proposal is recovered by a normalised kernel
+inverse: the predicted velocity is smoothed (sum K_0.25 v / sum K_0.25) and divided by the kernel mass
+sum_l K(x_k, x_l) of the deformation kernel, which inverts K for fields smooth at its width and applies unchanged at
+any mesh resolution.
+
+Training data: pairs generated by the method itself -- random smooth normal momentum fields a = (K_s z) n (z a
+scalar white-noise field, rescaled to an initial speed drawn in [vmin, vmax]) shot with the deformation kernel; the
+label is the normal part of the generating initial velocity.
+"""
+import math
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from . import pointEvolution as evol
+from .kernelFunctions import Kernel
+
+IN_DIM, HIDDEN, OUT_DIM, N_OUT = 64, 128, 64, 3
+N_FEATURES = 17
+VELOCITY_SCALE = 0.3
+ROW_PAD = 64
+
+
+def _pad_rows(n):
+    return ((n + ROW_PAD - 1) // ROW_PAD) * ROW_PAD
+
+
+def vertex_normals(X, faces_t):
+    """Area-weighted vertex normals (sum of incident face surfels, normalised)."""
+    v0, v1, v2 = X[faces_t[:, 0]], X[faces_t[:, 1]], X[faces_t[:, 2]]
+    s = torch.cross(v1 - v0, v2 - v0, dim=1) * 0.5
+    n = torch.zeros_like(X)
+    for j in range(3):
+        n.index_add_(0, faces_t[:, j], s)
+    return n / n.norm(dim=1, keepdim=True).clamp_min(1e-12)
+
+
+def nearest_displacement(X, Y):
+    D = torch.empty_like(X)
+    nat.check(nat.lib().lddmm_nearest_displacement(nat.ptr(X), X.shape[0], nat.ptr(Y), Y.shape[0], nat.ptr(D),
+                                                   nat.stream_ptr()), 'nearest_displacement')
+    return D
+
+
+_SMOOTH = {}
+
+
+def _smoother(sigma):
+    K = _SMOOTH.get(sigma)
+    if K is None:
+        K = Kernel(name='gauss', sigma=sigma)
+        K.pk_dtype = 'float32'
+        _SMOOTH[sigma] = K
+    return K
+
+
+def pair_features(X0, faces_t, X1, normals=None):
+    """(N, IN_DIM) bf16 feature matrix (rows padded to a multiple of 64 with zeros) for source X0 and target X1."""
+    n = X0.shape[0]
+    nrm = vertex_normals(X0, faces_t) if normals is None else normals
+    d = nearest_displacement(X0, X1)
+    ones = torch.ones_like(X0)
+    feats = [X0 - X0.mean(dim=0, keepdim=True), nrm, d]
+    for s in (0.25, 0.5):
+        K = _smoother(s)
+        feats.append(K.applyK(X0, d) / K.applyK(X0, ones))
+    feats.append((d * nrm).sum(dim=1, keepdim=True))
+    feats.append(d.norm(dim=1, keepdim=True))
+    F = torch.zeros((_pad_rows(n), IN_DIM), dtype=torch.bfloat16, device=X0.device)
+    F[:n, :N_FEATURES] = torch.cat(feats, dim=1).to(torch.bfloat16)
+    return F
+
+
+class MomentumProposal:
+    """Per-vertex MLP with hand-written BF16 forward / backward kernels and an Adam step kernel."""
+
+    dims = (IN_DIM, HIDDEN, HIDDEN, HIDDEN, OUT_DIM)
+
+    def __init__(self, seed=0, device='cuda'):
+        g = torch.Generator(device='cpu').manual_seed(seed)
+        self.W, self.b = [], []
+        for i in range(4):
+            fi, fo = self.dims[i], self.dims[i + 1]
+            w = torch.randn((fi, fo), generator=g, dtype=torch.float32) * math.sqrt(2.0 / fi)
+            if i == 0:
+                w[N_FEATURES:] = 0.0
+            if i == 3:
+                w *= 0.1
+                w[:, N_OUT:] = 0.0
+            self.W.append(w.to(device))
+            self.b.append(torch.zeros(fo, dtype=torch.float32, device=device))
+        self.Wb = [w.to(torch.bfloat16) for w in self.W]
+        self.m = [torch.zeros_like(t) for t in self.W + self.b]
+        self.v = [torch.zeros_like(t) for t in self.W + self.b]
+        self.step = 0
+
+    # ------------------------------------------------------------------ kernels
+    @staticmethod
+    def _gemm(ta, tb, epi, A, B, C, M, N, K, bias=None, mask=None, splits=1, split_ws=None):
+        sw, swb = (split_ws, split_ws.numel() * 4) if split_ws is not None else (None, 0)
+        nat.check(nat.lib().lddmm_bf16_gemm(ta, tb, epi, M, N, K, nat.ptr(A), nat.ptr(B), nat.ptr(bias),
+                                            nat.ptr(mask), nat.ptr(C), splits, nat.ptr(sw), swb, nat.stream_ptr()),
+                  'bf16_gemm')
+
+    def forward(self, F, keep=False):
+        """F (M, IN_DIM) bf16, M a multiple of 64 -> (M, 64) f32 outputs (and the activations when keep)."""
+        M = F.shape[0]
+        acts = [F]
+        h = F
+        for i in range(3):
+            out = torch.empty((M, self.dims[i + 1]), dtype=torch.bfloat16, device=F.device)
+            self._gemm(0, 0, 2, h, self.Wb[i], out, M, self.dims[i + 1], self.dims[i], bias=self.b[i])
+            acts.append(out)
+            h = out
+        y = torch.empty((M, OUT_DIM), dtype=torch.float32, device=F.device)
+        self._gemm(0, 0, 1, h, self.Wb[3], y, M, OUT_DIM, HIDDEN, bias=self.b[3])
+        return (y, acts) if keep else y
+
+    def gradients(self, F, target, valid, weight=None):
+        """Loss (device scalar) and FP32 gradients [dW0..dW3, db0..db3] of the mean squared error on the first 3
+        outputs of rows < valid (target (M,3) f32)."""
+        M = F.shape[0]
+        y, acts = self.forward(F, keep=True)
+        w = (1.0 / max(valid, 1)) if weight is None else weight
+        dy = torch.empty((M, OUT_DIM), dtype=torch.bfloat16, device=F.device)
+        row_loss = torch.empty(M, dtype=torch.float32, device=F.device)
+        nat.check(nat.lib().lddmm_mse_grad(nat.ptr(y), M, OUT_DIM, nat.ptr(target), N_OUT, int(valid), float(w),
+                                           nat.ptr(dy), nat.ptr(row_loss), nat.stream_ptr()), 'mse_grad')
+        splits = max(1, min(64, M // 2048))
+        split_ws = torch.empty(splits * HIDDEN * HIDDEN, dtype=torch.float32, device=F.device) if splits > 1 else None
+        dW, db = [None] * 4, [None] * 4
+        for i in range(3, -1, -1):
+            fi, fo = self.dims[i], self.dims[i + 1]
+            gw = torch.empty((fi, fo), dtype=torch.float32, device=F.device)
+            sp = splits if split_ws is not None and fi * fo <= HIDDEN * HIDDEN else 1
+            self._gemm(1, 0, 0, acts[i], dy, gw, fi, fo, M, splits=sp, split_ws=split_ws if sp > 1 else None)
+            gb = torch.empty(fo, dtype=torch.float32, device=F.device)
+            nat.check(nat.lib().lddmm_bf16_colsum(nat.ptr(dy), M, fo, nat.ptr(gb), nat.stream_ptr()), 'colsum')
+            dW[i], db[i] = gw, gb
+            if i > 0:
+                dx = torch.empty((M, fi), dtype=torch.bfloat16, device=F.device)
+                self._gemm(0, 1, 4, dy, self.Wb[i], dx, M, fi, fo, mask=acts[i])
+                dy = dx
+        loss = row_loss.sum() * w
+        return loss, dW + db
+
+    def adam(self, grads, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0):
+        self.step += 1
+        params = self.W + self.b
+        for k, (p, g) in enumerate(zip(params, grads)):
+            pb = self.Wb[k] if k < 4 else None
+            nat.check(nat.lib().lddmm_adam_step(nat.ptr(p), nat.ptr(g), nat.ptr(self.m[k]), nat.ptr(self.v[k]),
+                                                nat.ptr(pb), p.numel(), lr, beta1, beta2, eps, self.step,
+                                                weight_decay, nat.stream_ptr()), 'adam_step')
+
+    # ------------------------------------------------------------------ inference
+    def predict_velocity(self, X0, faces_t, X1, normals=None):
+        """Predicted initial velocity v0 (N,3) f64 for registering X0 (with faces) onto the target points X1."""
+        n = X0.shape[0]
+        F = pair_features(X0, faces_t, X1, normals)
+        y = self.forward(F)
+        return (y[:n, :N_OUT].to(torch.float64) * VELOCITY_SCALE).contiguous()
+
+    def predict(self, X0, faces_t, X1, Kdef, normals=None):
+        """Initial momentum proposal a0 (N,3) f64: the smoothed velocity divided by the kernel mass of Kdef."""
+        v = self.predict_velocity(X0, faces_t, X1, normals)
+        ones = torch.ones_like(X0)
+        Ks = _smoother(0.25)
+        v = Ks.applyK(X0, v) / Ks.applyK(X0, ones)
+        return (v / Kdef.applyK(X0, ones)).contiguous()
+
+    def state_dict(self):
+        return {'W': [w.cpu() for w in self.W], 'b': [b.cpu() for b in self.b], 'step': self.step}
+
+    def load_state_dict(self, d):
+        self.W = [w.cuda() for w in d['W']]
+        self.b = [b.cuda() for b in d['b']]
+        self.Wb = [w.to(torch.bfloat16) for w in self.W]
+        self.step = d.get('step', 0)
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Training data generated by the method itself, and training
+# ---------------------------------------------------------------------------------------------------------------
+def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, timeStep=0.1, vmin=0.05, vmax=0.35):
+    """Features (n_pairs, Mpad, IN_DIM) bf16, labels (n_pairs, Mpad, 3) f32 and momenta (n_pairs, n, 3) f64 of pairs
+    (x0, shoot(x0, a_i)).
+
+    a_i = (K_{sigma_smooth} z) n with z a scalar white-noise field, rescaled to an initial speed ~ U[vmin, vmax];
+    targets shot with K_{sigma_def} over round(1/timeStep) steps; labels are the normal parts of the initial
+    velocities K_{sigma_def}(x0) a_i, over VELOCITY_SCALE."""
+    X0 = nat.as_device(x0)
+    faces_t = torch.from_numpy(np.ascontiguousarray(faces, dtype=np.int64)).cuda()
+    n = X0.shape[0]
+    Mp = _pad_rows(n)
+    Kdef = Kernel(name='gauss', sigma=sigma_def)
+    Kdef.pk_dtype = 'float32'
+    Ksm = Kernel(name='gauss', sigma=sigma_smooth)
+    Ksm.pk_dtype = 'float32'
+    normals = vertex_normals(X0, faces_t)
+    gen = torch.Generator(device='cuda').manual_seed(seed)
+    speeds = torch.rand(n_pairs, generator=gen, dtype=torch.float64, device='cuda') * (vmax - vmin) + vmin
+    feats = torch.zeros((n_pairs, Mp, IN_DIM), dtype=torch.bfloat16, device='cuda')
+    labels = torch.zeros((n_pairs, Mp, N_OUT), dtype=torch.float32, device='cuda')
+    momenta = torch.zeros((n_pairs, n, 3), dtype=torch.float64, device='cuda')
+    origin = nat.centroid(X0)
+    for i in range(n_pairs):
+        z = torch.randn((n, 1), generator=gen, dtype=torch.float64, device='cuda').expand(n, 3).contiguous()
+        a = Ksm.applyK(X0, z)[:, :1] * normals
+        v = Kdef.applyK(X0, a)
+        scale = speeds[i] / v.norm(dim=1).max()
+        a, v = a * scale, v * scale
+        xt, _ = evol.shoot_second_order(X0, a, Kdef, timeStep, origin=origin)
+        feats[i] = pair_features(X0, faces_t, xt[-1], normals)
+        vn = (v * normals).sum(dim=1, keepdim=True) * normals
+        labels[i, :n] = (vn / VELOCITY_SCALE).to(torch.float32)
+        momenta[i] = a
+    return feats, labels, momenta, n
+
+
+def train(model, feats, labels, n, epochs=10, batch_pairs=16, lr=1e-3, seed=0, log=None):
+    """Minibatch Adam on (n_pairs, Mp, .) tensors; returns the per-epoch mean training loss."""
+    P, Mp = feats.shape[0], feats.shape[1]
+    gen = torch.Generator(device='cpu').manual_seed(seed)
+    history = []
+    for ep in range(epochs):
+        order = torch.randperm(P, generator=gen)
+        tot = torch.zeros((), dtype=torch.float64, device='cuda')
+        nb = 0
+        for s in range(0, P - batch_pairs + 1, batch_pairs):
+            idx = order[s:s + batch_pairs].cuda()
+            F = feats[idx].reshape(-1, IN_DIM)
+            T = labels[idx].reshape(-1, N_OUT)
+            # padding rows (zero features, zero label) stay in the batch: they only ask f(0) = 0
+            loss, grads = model.gradients(F, T, F.shape[0], weight=1.0 / (batch_pairs * Mp))
+            model.adam(grads, lr=lr)
+            tot += loss
+            nb += 1
+        history.append(float(tot) / max(nb, 1))
+        if log:
+            log(f'epoch {ep}: loss {history[-1]:.6f}')
+    return history
+
+
+def warm_start(matching, model):
+    """Set matching.control['a0'] to the network's proposal when it lowers the objective, else keep zero momentum
+    (the plain optimiser is the fallback). Returns (used_proposal, objective_at_proposal, objective_at_zero)."""
+    X0 = matching.x0
+    faces_t = matching.data.faces
+    a_prop = model.predict(X0, faces_t, matching.data.x1, matching.options['KparDiff'])
+    zero = torch.zeros_like(a_prop)
+    matching.obj = None
+    obj_zero = matching.objectiveFun() if torch.equal(matching.control['a0'], zero) else None
+    if obj_zero is None:
+        matching.control['a0'] = zero
+        matching.obj = None
+        obj_zero = matching.objectiveFun()
+    obj_prop = matching.updateTry({'a0': -a_prop}, 1.0)     # control - 1.0 * (-a_prop) = a_prop
+    used = bool(np.isfinite(obj_prop) and obj_prop < obj_zero)
+    if used:
+        matching.acceptVarTry()
+    return used, obj_prop, obj_zero
