@@ -16,6 +16,7 @@ Differences from the reference, by design:
   * affine parts, landmarks, symmetric / unreduced / SGD variants and file output are not implemented.
 """
 import logging
+import time
 from copy import deepcopy
 
 import numpy as np
@@ -31,6 +32,10 @@ from .surfaces import Surface
 
 class Control(dict):
     pass
+
+
+class TargetReached(Exception):
+    """Raised at the end of an iteration whose objective is at or below options['targetObjective']."""
 
 
 class State(dict):
@@ -57,7 +62,7 @@ class _DeviceMatching:
                 'affineKernel': False, 'testGradient': False, 'Landmarks': None, 'saveFile': 'evolution',
                 'saveRate': 10, 'mode': 'normal', 'verb': True, 'pplot': False, 'outputDir': '.',
                 'symmetric': False, 'internalCost': None, 'lineSearch': 'Weak_Wolfe', 'gradTol': -1.,
-                'gradLB': 0.001, 'initialMomentum': None}
+                'gradLB': 0.001, 'initialMomentum': None, 'targetObjective': None}
 
     def __init__(self, Template=None, Target=None, options=None):
         self.options = self.getDefaultOptions()
@@ -106,6 +111,7 @@ class _DeviceMatching:
         self.iter = 0
         self.pkBuffer = 0
         self.history = []
+        self.times = []
         self.control = Control()
         self.controlTry = Control()
         self.state = State()
@@ -191,10 +197,14 @@ class _DeviceMatching:
     def endOfIteration(self, endP=False):
         self.iter += 1
         self.history.append(self.obj)
+        self.times.append(time.perf_counter())
         if self.pkBuffer > 50:
             self.resetPK()
         else:
             self.pkBuffer += 1
+        target = self.options['targetObjective']
+        if target is not None and self.obj is not None and self.obj <= target and not endP:
+            raise TargetReached()
 
     def endOfProcedure(self):
         self.endOfIteration(endP=True)
@@ -209,9 +219,14 @@ class _DeviceMatching:
             self.gradEps = max(1e-5, np.sqrt(grd2) / 10000)
         self.epsMax = 5.
         logging.info(f'Gradient lower bound: {self.gradEps:.5f}')
-        _bfgs.bfgs(self, verb=self.options['verb'], maxIter=self.options['maxIter'],
-                   TestGradient=self.options['testGradient'], epsInit=self.options['epsInit'],
-                   Wolfe=self.options['Wolfe'], lineSearch=self.options['lineSearch'], memory=50)
+        self.reached_target = False
+        try:
+            _bfgs.bfgs(self, verb=self.options['verb'], maxIter=self.options['maxIter'],
+                       TestGradient=self.options['testGradient'], epsInit=self.options['epsInit'],
+                       Wolfe=self.options['Wolfe'], lineSearch=self.options['lineSearch'], memory=50)
+        except TargetReached:
+            self.reached_target = True
+            self.endOptim()
         return self.control
 
 
