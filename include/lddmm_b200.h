@@ -127,6 +127,19 @@ int lddmm_second_order_adjoint_step(const double* x, const double* a, const doub
                                     double* pa_prev, int precision, void* workspace, size_t workspace_bytes,
                                     lddmm_stream_t stream);
 
+/* Row-range forms for sharding one time step over several GPUs (targets = rows row0 .. row0+nrows-1 of the full
+ * state, sources = all n rows; outputs are the nrows new rows). Same sums as the whole-step entry points above
+ * (base/pointEvolution.py:433-449 and :539-546); workspace: lddmm_workspace_bytes(nrows, n, precision). */
+int lddmm_second_order_step_rows(const double* x, const double* a, int64_t n, int64_t row0, int64_t nrows,
+                                 double sigma, double dt, const double* origin, double* x_next_rows,
+                                 double* a_next_rows, int precision, void* workspace, size_t workspace_bytes,
+                                 lddmm_stream_t stream);
+int lddmm_second_order_adjoint_step_rows(const double* x, const double* a, const double* px, const double* pa,
+                                         int64_t n, int64_t row0, int64_t nrows, double sigma, double dt,
+                                         const double* origin, double* px_prev_rows, double* pa_prev_rows,
+                                         int precision, void* workspace, size_t workspace_bytes,
+                                         lddmm_stream_t stream);
+
 /* Full adjoint sweep + gradient: given xt, at (T+1,n,3) and px1, pa1 (n,3), writes pxt, pat (T+1,n,3) and
  * da0 = K(x0) a0 - pat[0].  secondOrderCovector / secondOrderGradient  base/pointEvolution.py:489-618. */
 int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, double dt,

@@ -38,6 +38,9 @@ SIGNATURES = {
     'lddmm_apply_diff_k_mat': [_dp, _i64, _dp, _i64, _dp, _f64, _dp, _vp],
     'lddmm_second_order_step': [_dp, _dp, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
     'lddmm_second_order_shoot': [_dp, _dp, _i64, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_second_order_step_rows': [_dp, _dp, _i64, _i64, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_second_order_adjoint_step_rows': [_dp, _dp, _dp, _dp, _i64, _i64, _i64, _f64, _f64, _hp, _dp, _dp,
+                                             _int, _vp, _sz, _vp],
     'lddmm_second_order_adjoint_step': [_dp, _dp, _dp, _dp, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
     'lddmm_second_order_gradient': [_dp, _dp, _i64, _i64, _f64, _f64, _dp, _dp, _hp, _dp, _dp, _dp, _int, _vp, _sz,
                                     _vp],

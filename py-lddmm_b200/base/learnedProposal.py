@@ -87,6 +87,24 @@ def pair_features(X0, faces_t, X1, normals=None):
     return F
 
 
+def kernel_cg(K, X, b, a0, iters):
+    """`iters` conjugate-gradient steps on K(X) a = b from a0 (K symmetric positive definite); every product is one
+    kernel sum in the library, the scalars stay on the device (no host synchronisation)."""
+    a = a0.clone()
+    r = b - K.applyK(X, a)
+    p = r.clone()
+    rr = (r * r).sum()
+    for _ in range(iters):
+        q = K.applyK(X, p)
+        alpha = rr / (p * q).sum().clamp_min(1e-300)
+        a = a + alpha * p
+        r = r - alpha * q
+        rr_new = (r * r).sum()
+        p = r + (rr_new / rr.clamp_min(1e-300)) * p
+        rr = rr_new
+    return a
+
+
 class MomentumProposal:
     """Per-vertex MLP with hand-written BF16 forward / backward kernels and an Adam step kernel."""
 
@@ -177,13 +195,18 @@ class MomentumProposal:
         y = self.forward(F)
         return (y[:n, :N_OUT].to(torch.float64) * VELOCITY_SCALE).contiguous()
 
-    def predict(self, X0, faces_t, X1, Kdef, normals=None):
-        """Initial momentum proposal a0 (N,3) f64: the smoothed velocity divided by the kernel mass of Kdef."""
+    def predict(self, X0, faces_t, X1, Kdef, normals=None, cg_iters=0):
+        """Initial momentum proposal a0 (N,3) f64: the smoothed predicted velocity v divided by the kernel mass of
+        Kdef, optionally refined by `cg_iters` conjugate-gradient steps on K(x0) a = v (early stopping keeps the
+        kernel inverse from amplifying the prediction's vertex-level noise)."""
         v = self.predict_velocity(X0, faces_t, X1, normals)
         ones = torch.ones_like(X0)
         Ks = _smoother(0.25)
         v = Ks.applyK(X0, v) / Ks.applyK(X0, ones)
-        return (v / Kdef.applyK(X0, ones)).contiguous()
+        a = v / Kdef.applyK(X0, ones)
+        if cg_iters > 0:
+            a = kernel_cg(Kdef, X0, v, a, cg_iters)
+        return a.contiguous()
 
     def state_dict(self):
         return {'W': [w.cpu() for w in self.W], 'b': [b.cpu() for b in self.b], 'step': self.step}
@@ -258,12 +281,12 @@ def train(model, feats, labels, n, epochs=10, batch_pairs=16, lr=1e-3, seed=0, l
     return history
 
 
-def warm_start(matching, model):
+def warm_start(matching, model, cg_iters=0):
     """Set matching.control['a0'] to the network's proposal when it lowers the objective, else keep zero momentum
     (the plain optimiser is the fallback). Returns (used_proposal, objective_at_proposal, objective_at_zero)."""
     X0 = matching.x0
     faces_t = matching.data.faces
-    a_prop = model.predict(X0, faces_t, matching.data.x1, matching.options['KparDiff'])
+    a_prop = model.predict(X0, faces_t, matching.data.x1, matching.options['KparDiff'], cg_iters=cg_iters)
     zero = torch.zeros_like(a_prop)
     matching.obj = None
     obj_zero = matching.objectiveFun() if torch.equal(matching.control['a0'], zero) else None

@@ -9,6 +9,8 @@ namespace lddmm {
 // Second-order forward step (secondOrderEvolution loop body, base/pointEvolution.py:433-449):
 //   x1 = x + dt K(x) a,   a1 = a + dt za with za = -DK^T(x; a, a) = kappa sum_l e (a_k.a_l) d.
 // Accumulators: X = sum e a_l (3), A = sum e (a_k.a_l) d (3). 16 FP32 + 1 SFU per pair.
+// Targets are the rows row0 .. row0+n-1 of (x, a) (row0 = 0 and n = m for a whole step; a row range for the
+// sharded step), sources all m rows; outputs x1, a1 are indexed by the local target index.
 struct OpSOFwd {
   static constexpr int NS = 6, NA = 6;
   struct Params {
@@ -16,10 +18,13 @@ struct OpSOFwd {
     double *x1, *a1;
     Frame f;
     double dt;
+    int row0 = 0;
   };
   template <typename V> struct Tgt { V y0, y1, y2, a0, a1, a2; };
   template <typename V>
   static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
+    i0 += P.row0;
+    i1 += P.row0;
     t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
     t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
     t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
@@ -45,9 +50,10 @@ struct OpSOFwd {
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double ka = P.dt * P.f.kappa;
+    const int g = P.row0 + i;
     for (int c = 0; c < 3; ++c) {
-      P.x1[3 * i + c] = P.x[3 * i + c] + P.dt * acc[c];
-      P.a1[3 * i + c] = P.a[3 * i + c] + ka * acc[3 + c];
+      P.x1[3 * i + c] = P.x[3 * g + c] + P.dt * acc[c];
+      P.a1[3 * i + c] = P.a[3 * g + c] + ka * acc[3 + c];
     }
   }
 };
@@ -60,6 +66,8 @@ struct OpSOFwd {
 //   G = sum e (c1' + c2'' dq) d (3), C = sum e c2'' (1), D = sum e c2'' pa_l (3), E = sum e px'_l (3),
 //   F = sum e dq a_l (3)
 // and zpx = G + (pa_k C - D)/(sigma^2 (-kappa^2)), zpa = E/(-kappa) + kappa F. 38 FP32 + 1 SFU per pair.
+// Targets are rows row0 .. row0+n-1 of the state and covectors (row0 = 0 for a whole step), sources all rows;
+// outputs px_prev, pa_prev are indexed by the local target index.
 struct OpSOBwd {
   static constexpr int NS = 12, NA = 13;
   struct Params {
@@ -67,11 +75,14 @@ struct OpSOBwd {
     double *px_prev, *pa_prev;
     Frame f;
     double dt;
+    int row0 = 0;
   };
   template <typename V> struct Tgt { V y0, y1, y2, a0, a1, a2, b0, b1, b2, p0, p1, p2, q0, q1, q2; };
   template <typename V>
   static __device__ __forceinline__ void load_target(const Params& P, int i0, int i1, Tgt<V>& t) {
     const double k = P.f.kappa;
+    i0 += P.row0;
+    i1 += P.row0;
     t.y0 = tgt_coord<V>(P.x, i0, i1, 0, P.f.o0, P.f.s);
     t.y1 = tgt_coord<V>(P.x, i0, i1, 1, P.f.o1, P.f.s);
     t.y2 = tgt_coord<V>(P.x, i0, i1, 2, P.f.o2, P.f.s);
@@ -125,11 +136,12 @@ struct OpSOBwd {
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = P.f.kappa;
     const double cd = -1.0 / (k * k) * P.f.inv_s2;  // converts the c2''-weighted sums back, times 1/sigma^2
+    const int g = P.row0 + i;
     for (int c = 0; c < 3; ++c) {
-      const double pa = P.pa[3 * i + c];
+      const double pa = P.pa[3 * g + c];
       const double zpx = acc[c] + cd * (pa * acc[3] - acc[4 + c]);
       const double zpa = -acc[7 + c] / k + k * acc[10 + c];
-      P.px_prev[3 * i + c] = P.px[3 * i + c] + P.dt * zpx;
+      P.px_prev[3 * i + c] = P.px[3 * g + c] + P.dt * zpx;
       P.pa_prev[3 * i + c] = pa + P.dt * zpa;
     }
   }
@@ -257,16 +269,17 @@ int k_energy_and_update(const double* x, const double* a, int64_t n, const Frame
 
 template <typename V>
 int so_step(const double* x, const double* a, int64_t n, const Frame& f, double dt, double* x1, double* a1, void* ws,
-            size_t wsb, cudaStream_t st) {
-  OpSOFwd::Params P{x, a, x1, a1, f, dt};
-  return run_pairs<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
+            size_t wsb, cudaStream_t st, int64_t row0 = 0, int64_t nrows = -1) {
+  OpSOFwd::Params P{x, a, x1, a1, f, dt, (int)row0};
+  return run_pairs<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
 }
 
 template <typename V>
 int so_adjoint_step(const double* x, const double* a, const double* px, const double* pa, int64_t n, const Frame& f,
-                    double dt, double* px_prev, double* pa_prev, void* ws, size_t wsb, cudaStream_t st) {
-  OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt};
-  return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH>(P, n, n, ws, wsb, st);
+                    double dt, double* px_prev, double* pa_prev, void* ws, size_t wsb, cudaStream_t st,
+                    int64_t row0 = 0, int64_t nrows = -1) {
+  OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt, (int)row0};
+  return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
 }
 
 template <typename V>
@@ -357,6 +370,21 @@ int lddmm_second_order_step(const double* x, const double* a, int64_t n, double 
                         so_step<double>(x, a, n, frame<double>(origin, sigma), dt, x_next, a_next, ws, wsb, st));
 }
 
+int lddmm_second_order_step_rows(const double* x, const double* a, int64_t n, int64_t row0, int64_t nrows,
+                                 double sigma, double dt, const double* origin, double* x_next_rows,
+                                 double* a_next_rows, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || row0 < 0 || nrows < 0 || row0 + nrows > n || bad_sigma(sigma) || bad(x, n) || bad(a, n) ||
+      bad(x_next_rows, nrows) || bad(a_next_rows, nrows))
+    return kInvalidArgument;
+  if (nrows == 0) return kOk;
+  cudaStream_t st = (cudaStream_t)stream;
+  return LDDMM_DISPATCH(precision,
+                        so_step<F2>(x, a, n, frame<F2>(origin, sigma), dt, x_next_rows, a_next_rows, ws, wsb, st,
+                                    row0, nrows),
+                        so_step<double>(x, a, n, frame<double>(origin, sigma), dt, x_next_rows, a_next_rows, ws, wsb,
+                                        st, row0, nrows));
+}
+
 int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int64_t T, double sigma, double dt,
                              const double* origin, double* xt, double* at, int precision, void* ws, size_t wsb,
                              lddmm_stream_t stream) {
@@ -377,6 +405,22 @@ int lddmm_second_order_adjoint_step(const double* x, const double* a, const doub
   return LDDMM_DISPATCH(
       precision, so_adjoint_step<F2>(x, a, px, pa, n, frame<F2>(origin, sigma), dt, px_prev, pa_prev, ws, wsb, st),
       so_adjoint_step<double>(x, a, px, pa, n, frame<double>(origin, sigma), dt, px_prev, pa_prev, ws, wsb, st));
+}
+
+int lddmm_second_order_adjoint_step_rows(const double* x, const double* a, const double* px, const double* pa,
+                                         int64_t n, int64_t row0, int64_t nrows, double sigma, double dt,
+                                         const double* origin, double* px_prev_rows, double* pa_prev_rows,
+                                         int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || row0 < 0 || nrows < 0 || row0 + nrows > n || bad_sigma(sigma) || bad(x, n) || bad(a, n) ||
+      bad(px, n) || bad(pa, n) || bad(px_prev_rows, nrows) || bad(pa_prev_rows, nrows))
+    return kInvalidArgument;
+  if (nrows == 0) return kOk;
+  cudaStream_t st = (cudaStream_t)stream;
+  return LDDMM_DISPATCH(precision,
+                        so_adjoint_step<F2>(x, a, px, pa, n, frame<F2>(origin, sigma), dt, px_prev_rows,
+                                            pa_prev_rows, ws, wsb, st, row0, nrows),
+                        so_adjoint_step<double>(x, a, px, pa, n, frame<double>(origin, sigma), dt, px_prev_rows,
+                                                pa_prev_rows, ws, wsb, st, row0, nrows));
 }
 
 int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, double dt,

@@ -109,3 +109,60 @@ def test_first_order_energy_and_euclidean_gradient():
     for t in range(T):
         g = 2 * 0.8 * d['at'][t] - d['pxt'][t + 1]
         assert rel_err(dat[t].cpu().numpy(), O.apply_k(d['xt'][t], d['xt'][t], g, 0.5)) < 1e-11
+
+
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+def test_row_range_steps_match_whole_steps(dtype):
+    """lddmm_second_order_step_rows / _adjoint_step_rows on a row range equal the same rows of the whole step."""
+    import torch
+    from base import distributed as dd
+    from base import _native as nat
+    from base import pointEvolution as evol
+    from base.syntheticShapes import icosphere
+    x0, _ = icosphere(4)
+    rng = np.random.default_rng(8)
+    X = torch.from_numpy(x0).cuda()
+    A = torch.from_numpy(rng.normal(0, 0.01, x0.shape)).cuda()
+    PX = torch.from_numpy(rng.normal(size=x0.shape)).cuda()
+    PA = torch.from_numpy(rng.normal(0, 0.1, x0.shape)).cuda()
+    K = kernel(0.5, dtype)
+    o = nat.centroid(X)
+    xt, at = evol.shoot_second_order(X, A, K, 0.5, origin=o)            # two steps of size 0.5
+    step = dd.library_step_rows(K, o)
+    adj = dd.library_adjoint_rows(K, o)
+    tol = 1e-6 if dtype == 'float32' else 1e-13
+    for r0, r1 in ((0, x0.shape[0]), (100, 1300), (2000, 2562)):
+        x1, a1 = step(X, A, r0, r1, 0.5)
+        assert rel_err(x1.cpu().numpy(), xt[1, r0:r1].cpu().numpy()) < tol
+        assert rel_err(a1.cpu().numpy(), at[1, r0:r1].cpu().numpy()) < tol
+    pxt, pat, _ = evol.second_order_adjoint(xt, at, PX, PA, K, 0.5, origin=o, with_da0=False)
+    for r0, r1 in ((0, x0.shape[0]), (7, 901)):
+        p0, q0 = adj(xt[1], at[1], PX, PA, r0, r1, 0.5)
+        assert rel_err(p0.cpu().numpy(), pxt[1, r0:r1].cpu().numpy()) < tol
+        assert rel_err(q0.cpu().numpy(), pat[1, r0:r1].cpu().numpy()) < tol
+
+
+def test_sharded_shooting_nccl_single_rank():
+    """The NCCL code path of the sharded driver on one GPU (world size 1) reproduces the unsharded trajectory."""
+    import os
+    import torch
+    import torch.distributed as dist
+    from base import distributed as dd
+    from base import pointEvolution as evol
+    from base import _native as nat
+    from base.syntheticShapes import icosphere
+    x0, _ = icosphere(3)
+    X = torch.from_numpy(x0).cuda()
+    A = torch.from_numpy(np.random.default_rng(9).normal(0, 0.01, x0.shape)).cuda()
+    K = kernel(0.5, 'float32')
+    o = nat.centroid(X)
+    os.environ.setdefault('MASTER_ADDR', '127.0.0.1')
+    os.environ.setdefault('MASTER_PORT', str(29400 + os.getpid() % 500))
+    dist.init_process_group('nccl', rank=0, world_size=1)
+    try:
+        xt, at = dd.sharded_second_order_shoot(X, A, 0.1, dd.library_step_rows(K, o))
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    rx, ra = evol.shoot_second_order(X, A, K, 0.1, origin=o)
+    assert torch.equal(xt, rx) and torch.equal(at, ra)
