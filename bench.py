@@ -16,6 +16,10 @@ compensated accumulation and FP64 outputs.
 `--impl reference` times the CPU implementation of the same sums (the oracle restatement of the reference's
 numba kernels, all host threads) and prints the same metric with "impl": "reference".
 
+  registration  (1 GPU) seconds per registration pair to reach 1e-3 relative energy of the FP64 plain optimum on
+            the level-6 problem: plain FP64 path, FP32 path, FP32 path + learned warm start (the other half of the
+            headline metric); skipped with --no-registration
+
 Multi-GPU (torchrun): every rank runs the same workload on its own GPU (independent replicas, weak scaling);
 times are the max over ranks; value = pairs of all ranks / that time.
 """
@@ -198,6 +202,75 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# E* of the L6 registration below: FP64 plain path (pk_dtype float64, zero initial momentum) run to the reference's
+# BFGS stopping rule (108 iterations, |obj - obj_old| < 1e-7); `--recompute-estar` re-derives it.
+L6_ESTAR = 0.12269117945467034
+
+
+def run_registration(args):
+    """Seconds per registration pair to reach (E - E*)/E* <= 1e-3 on the level-6 icosphere -> bumpy ellipsoid problem
+    (Gaussian sigma 0.5, varifold sigma 0.2, T = 20, sigmaError 1, BFGS): plain FP64 path vs FP32 path vs FP32 path with
+    the learned warm start (network trained here, at level 4, on pairs generated by shooting)."""
+    import torch
+    from base import learnedProposal as lp
+    from base.kernelFunctions import Kernel
+    from base.surfaceMatching import SecondOrderSurfaceMatching
+    from base.surfaces import Surface
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    level = args.reg_level
+    x0, F = icosphere(level)
+    x1 = bumpy_ellipsoid(x0, seed=0)
+
+    def solve(dtype, target=None, model=None, maxIter=600):
+        K = Kernel(name='gauss', sigma=0.5)
+        K.pk_dtype = dtype
+        opts = dict(maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=K, KparDist=('gauss', 0.2), sigmaError=1.0,
+                    errorType='varifold', pk_dtype=dtype, algorithm='bfgs', timeStep=0.05, verb=False,
+                    targetObjective=target)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
+        used = lp.warm_start(f, model) if model is not None else None
+        f.optimizeMatching()
+        torch.cuda.synchronize()
+        return f, time.perf_counter() - t0, used
+
+    res = {'problem': f'icosphere L{level} ({x0.shape[0]} vertices) -> bumpy ellipsoid, sigma 0.5 / varifold 0.2, '
+                      'T=20, sigmaError 1, BFGS', 'criterion': '(E - E*)/E* <= 1e-3'}
+    if args.recompute_estar or level != 6:
+        f64, t, _ = solve('float64')
+        estar = f64.history[-1]
+        res['estar_run'] = {'iters': len(f64.history), 's': t}
+    else:
+        estar = L6_ESTAR
+    res['estar'] = estar
+    target = estar * (1 + 1e-3)
+    t0 = time.perf_counter()
+    xs, Fs = icosphere(4)
+    feats, labels, _, n4 = lp.generate_pairs(xs, Fs, args.train_pairs, seed=0, timeStep=0.1)
+    model = lp.MomentumProposal(seed=0)
+    ntr = int(0.9 * args.train_pairs)
+    hist = lp.train(model, feats[:ntr], labels[:ntr], n4, epochs=args.train_epochs, batch_pairs=16, lr=2e-3)
+    with torch.no_grad():
+        y = model.forward(feats[ntr:].reshape(-1, lp.IN_DIM)).reshape(-1, feats.shape[1], lp.OUT_DIM)[:, :n4, :3]
+    res['proposal'] = {'train_pairs': ntr, 'heldout_pairs': args.train_pairs - ntr, 'epochs': args.train_epochs,
+                       'train_s': time.perf_counter() - t0, 'loss_first_last': [hist[0], hist[-1]],
+                       'heldout_velocity_rel_err': float((y - labels[ntr:, :n4]).norm() / labels[ntr:, :n4].norm())}
+    for name, dtype, model_ in (('plain_fp64', 'float64', None), ('plain_fp32', 'float32', None),
+                                ('learned_fp32', 'float32', model)):
+        f, t, used = solve(dtype, target=target, model=model_)
+        f.resetPK('float64')
+        f.obj = None
+        e = f.objectiveFun()
+        res[name] = {'s_per_pair': t, 'iters': len(f.history), 'reached': bool(f.reached_target),
+                     'rel_energy_fp64': (e - estar) / abs(estar)}
+        if used is not None:
+            res[name].update({'proposal_used': used[0], 'obj_proposal': used[1], 'obj_zero': used[2]})
+    res['speedup_learned_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['learned_fp32']['s_per_pair']
+    res['speedup_plain_fp32_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['plain_fp32']['s_per_pair']
+    return res
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -322,6 +395,8 @@ def run_b200(args, rank, world, local_rank):
         'clocks': clocks, 'gpu_launches': launches,
         'pairs_per_step': pairs_per_step,
     }
+    if world == 1 and not args.no_registration:
+        line['registration'] = run_registration(args)
     print(json.dumps(line), flush=True)
 
 
@@ -333,6 +408,11 @@ def main():
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-targets', type=int, default=4096)
     ap.add_argument('--ref-targets', type=int, default=2048)
+    ap.add_argument('--no-registration', action='store_true', help='skip the end-to-end registration measurement')
+    ap.add_argument('--recompute-estar', action='store_true')
+    ap.add_argument('--reg-level', type=int, default=6)
+    ap.add_argument('--train-pairs', type=int, default=2000)
+    ap.add_argument('--train-epochs', type=int, default=20)
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
