@@ -9,7 +9,8 @@ compensated accumulation and FP64 outputs.
             by writing a 256 MiB buffer; the flush is outside the timed events)
   e2e       the same step through the reference-facing API `Kernel.applyK(x, a)` with numpy (host) arrays:
             host->device copy of x and a, the kernels, device->host copy of the result, every step
-  roofline  the pair kernel against the FP32 pipe: 9 FP32 lane-ops + 1 SFU op per pair (see DESIGN.md);
+  roofline  the pair kernel against the FP32 pipe: 9 FP32 lane-ops + 1 SFU op per pair (3 differences,
+            3 FMAs for the scaled squared distance, 3 FMAs accumulating K a, one ex2);
             peak = 148 SMs x 128 FP32 lanes x max SM clock
   cpu_baseline  the CPU oracle (numba, float64, all host threads) on a bounded sample of the same sums
 
@@ -268,7 +269,33 @@ def run_registration(args):
             res[name].update({'proposal_used': used[0], 'obj_proposal': used[1], 'obj_zero': used[2]})
     res['speedup_learned_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['learned_fp32']['s_per_pair']
     res['speedup_plain_fp32_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['plain_fp32']['s_per_pair']
+    res['level4_fp64_50it'] = run_level4_fp64()
     return res
+
+
+def run_level4_fp64():
+    """The small CPU-runnable registration end to end: level-4 icosphere -> bumpy ellipsoid, sigma 0.5, varifold 0.3,
+    sigmaError 1, T = 10, BFGS, 50 iterations, float64 (the FP64 path, both matching classes)."""
+    import torch
+    from base.kernelFunctions import Kernel
+    from base.surfaceMatching import SurfaceMatching, SecondOrderSurfaceMatching
+    from base.surfaces import Surface
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    x0, F = icosphere(4)
+    x1 = bumpy_ellipsoid(x0, seed=0)
+    out = {}
+    for name, cls in (('second_order', SecondOrderSurfaceMatching), ('first_order', SurfaceMatching)):
+        K = Kernel(name='gauss', sigma=0.5)
+        K.pk_dtype = 'float64'
+        opts = dict(maxIter=50, affine='none', regWeight=1.0, KparDiff=K, KparDist=('gauss', 0.3), sigmaError=1.0,
+                    errorType='varifold', pk_dtype='float64', algorithm='bfgs', timeStep=0.1, verb=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = cls(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
+        f.optimizeMatching()
+        torch.cuda.synchronize()
+        out[name] = {'s': time.perf_counter() - t0, 'iters': len(f.history), 'final_obj': f.history[-1]}
+    return out
 
 
 def run_b200(args, rank, world, local_rank):

@@ -199,8 +199,8 @@ int lddmm_vertex_face_table(const int64_t* faces_host, int64_t nf, int64_t nv, i
                             int32_t* vf_items_host);
 
 /* ---------------------------------------------------------------------------------------------------------
- * Learned momentum proposal (north_star "learned part"; no counterpart in the reference, which has no learned
- * component). Per-vertex MLP with BF16 weights / activations and FP32 accumulation on the tensor cores.
+ * Learned momentum proposal (no counterpart in the reference, which has no learned component). Per-vertex MLP
+ * with BF16 weights / activations and FP32 accumulation on the tensor cores.
  * ------------------------------------------------------------------------------------------------------- */
 
 /* C = epilogue(op(A) op(B)): A is (M,K) row-major, or stored transposed (K,M) when trans_a; B is (K,N) row-major, or

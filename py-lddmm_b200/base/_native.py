@@ -163,7 +163,11 @@ def as_device(a, device=None, dtype=torch.float64):
 
 
 def centroid(t):
-    """Host-side centre used as the FP32 origin (translation-invariant results)."""
+    """Centre used as the FP32 origin (results are translation invariant). Host arrays are averaged on the host;
+    device tensors with one reduction (and one synchronisation)."""
+    if not isinstance(t, torch.Tensor):
+        a = np.asarray(t, dtype=np.float64).reshape(-1, 3)
+        return None if a.size == 0 else a.mean(axis=0).tolist()
     if t.numel() == 0:
         return None
     return t.reshape(-1, 3).mean(dim=0).tolist()

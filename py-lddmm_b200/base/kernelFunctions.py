@@ -105,10 +105,11 @@ class Kernel(KernelSpec):
         squeeze = A.dim() == 1
         if squeeze:
             A = A[:, None]
+        origin = nat.centroid(x)
         if A.shape[1] != 3:
-            r = self._multi(lambda s: self._k_generic(Y, X, A, s))
+            r = self._multi(lambda s: self._k_generic(Y, X, A, s, origin))
         else:
-            r = self._multi(lambda s: self._apply_k(Y, X, A, s))
+            r = self._multi(lambda s: self._apply_k(Y, X, A, s, origin))
         if squeeze:
             r = r[:, 0]
         return _out(r, like_np)
@@ -122,7 +123,7 @@ class Kernel(KernelSpec):
                                           self.precision, ws, wsb, nat.stream_ptr()), 'applyK')
         return out
 
-    def _k_generic(self, Y, X, A, sigma):
+    def _k_generic(self, Y, X, A, sigma, origin=None):
         """K a for momenta of any width d: columns in groups of 3 (zero padded)."""
         d = A.shape[1]
         cols = []
@@ -130,7 +131,7 @@ class Kernel(KernelSpec):
             blk = A[:, c0:c0 + 3]
             if blk.shape[1] < 3:
                 blk = torch.cat([blk, blk.new_zeros(blk.shape[0], 3 - blk.shape[1])], dim=1)
-            cols.append(self._apply_k(Y, X, blk.contiguous(), sigma))
+            cols.append(self._apply_k(Y, X, blk.contiguous(), sigma, origin))
         return torch.cat(cols, dim=1)[:, :d].contiguous()
 
     def _k_mat(self, Y, X, U, sigma):

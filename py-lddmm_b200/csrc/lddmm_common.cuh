@@ -22,6 +22,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#ifndef LDDMM_MIN_CTAS
+#define LDDMM_MIN_CTAS 1  // minimum resident CTAs per SM requested from ptxas (caps registers when > 1)
+#endif
+#ifndef LDDMM_SOURCE_UNROLL
+#define LDDMM_SOURCE_UNROLL 4  // unroll depth of the per-source loop over a shared-memory tile
+#endif
+
 namespace lddmm {
 
 enum Status : int {
@@ -35,6 +42,8 @@ enum Status : int {
 };
 
 enum Precision : int { kFP32Compensated = 0, kFP64 = 1 };
+
+constexpr int kSourceUnroll = LDDMM_SOURCE_UNROLL;
 
 // ---------------------------------------------------------------------------------------------------------
 // Packed FP32 pair (two lanes in one 64-bit register pair) and its arithmetic (PTX .f32x2, sm_100a).
@@ -225,8 +234,9 @@ inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int 
 // Output: ws[(slot * NA + c) * n + i] = compensated partial of accumulator c of target i for one segment.
 // ---------------------------------------------------------------------------------------------------------
 template <class Op, typename V, int TPB, int RT>
-__global__ void __launch_bounds__(TPB) pairs_kernel(const typename Op::Params P, int n, int m, int TT, long long W,
-                                                    int C, typename VT<V>::Partial* __restrict__ ws) {
+__global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
+    pairs_kernel(const typename Op::Params P, int n, int m, int TT, long long W, int C,
+                 typename VT<V>::Partial* __restrict__ ws) {
   constexpr int L = VT<V>::kLanes;
   constexpr int G = RT / L;  // lane groups per thread
   constexpr int NU = (Op::NS + 1) / 2;
@@ -276,7 +286,7 @@ __global__ void __launch_bounds__(TPB) pairs_kernel(const typename Op::Params P,
       for (int g = 0; g < G; ++g)
 #pragma unroll
         for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<V>::zero();
-#pragma unroll 4
+#pragma unroll kSourceUnroll
       for (int jj = 0; jj < TPB; ++jj) {
         V s[2 * NU];
 #pragma unroll
