@@ -325,8 +325,8 @@ def run_b200(args, rank, world, local_rank):
         for i, s in enumerate(SIGMAS):
             if evs is not None:
                 evs[i][0].record(stream)
-            rc = lib.lddmm_apply_k(nat.ptr(X), n, nat.ptr(X), nat.ptr(A), n, s, o, nat.ptr(outs[i]), nat.FP32C, ws,
-                                   wsb, sp)
+            rc = lib.lddmm_apply_k(nat.ptr(X), n, nat.ptr(X), nat.ptr(A), n, s, nat.KERNEL_GAUSS, o, nat.ptr(outs[i]),
+                                   nat.FP32C, ws, wsb, sp)
             if evs is not None:
                 evs[i][1].record(stream)
             if rc != 0:

@@ -39,6 +39,13 @@ enum {
 
 enum { LDDMM_FP32C = 0, LDDMM_FP64 = 1 };
 
+/* Kernel family (`kernel` argument): the Gaussian exp(-r^2 / (2 sigma^2)) (KernelSpec name 'gauss'), or the
+ * reference's 'laplacian' kernel of order q = 0..4, P_q(r / sigma) exp(-r / sigma) with the polynomials lapPol /
+ * lapPolDiff / lapPolDiff2 of base/kernelFunctions_util.py:20-56 (KernelSpec(name='laplacian', order=q),
+ * base/kernelFunctions.py:363-368). */
+enum { LDDMM_KERNEL_GAUSS = 0, LDDMM_KERNEL_LAPLACIAN_0 = 16, LDDMM_KERNEL_LAPLACIAN_4 = 20 };
+#define LDDMM_KERNEL_LAPLACIAN(order) (LDDMM_KERNEL_LAPLACIAN_0 + (order))
+
 /* Library version and self description. */
 const char* lddmm_version(void);
 const char* lddmm_status_string(int status);
@@ -49,40 +56,41 @@ size_t lddmm_workspace_bytes(int64_t n_max, int64_t m_max, int precision);
 /* ---------------------------------------------------------------------------------------------------------
  * Kernel operators (replace Kernel.* in base/kernelFunctions.py:452-674 and the numba / pykeops backends
  * ku.applyK / applyDiffKT / applyDDiffK / applykdiff1and2 / applyDiv / applyktensor in
- * base/kernelFunctions_util.py:443-1506). y: (n,3) targets, x: (m,3) sources.
+ * base/kernelFunctions_util.py:443-1506). y: (n,3) targets, x: (m,3) sources. `kernel`: LDDMM_KERNEL_GAUSS or
+ * LDDMM_KERNEL_LAPLACIAN(order) (LDDMM_ERR_INVALID_ARGUMENT otherwise).
  * ------------------------------------------------------------------------------------------------------- */
 
 /* out(n,3) = K(y, x) a.  Kernel.applyK(x, a, firstVar=y)  base/kernelFunctions.py:452. */
-int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
+int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma, int kernel,
                   const double* origin, double* out, int precision, void* workspace, size_t workspace_bytes,
                   lddmm_stream_t stream);
 
 /* out(n,3) = DK^T.  Kernel.applyDiffKT(x, p, a, firstVar=y, regweight, lddmm, sym)  base/kernelFunctions.py:581.
  * mode 0 = plain (p: (n,3), a: (m,3)); 1 = sym; 2 = lddmm (sym / lddmm need n == m, p and a both (n,3)). */
-int lddmm_apply_diff_kt(const double* y, int64_t n, const double* x, const double* p, const double* a,
-                        int64_t m, double sigma, int mode, double regweight, const double* origin, double* out,
+int lddmm_apply_diff_kt(const double* y, int64_t n, const double* x, const double* p, const double* a, int64_t m,
+                        double sigma, int kernel, int mode, double regweight, const double* origin, double* out,
                         int precision, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* out(n,3) = DDK_{11 and 12}(x; nn, a, p).  Kernel.applyDDiffK11and12(x, n, a, p)  base/kernelFunctions.py:665. */
 int lddmm_apply_ddiff_k11and12(const double* x, const double* nn, const double* a, const double* p, int64_t n,
-                               double sigma, const double* origin, double* out, int precision, void* workspace,
-                               size_t workspace_bytes, lddmm_stream_t stream);
+                               double sigma, int kernel, const double* origin, double* out, int precision,
+                               void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* out(n,3) = DK_{1 and 2}(x; a1, a2).  Kernel.applyDiffK1and2(x, a1, a2)  base/kernelFunctions.py:549. */
-int lddmm_apply_diff_k1and2(const double* x, const double* a1, const double* a2, int64_t n, double sigma,
-                            const double* origin, double* out, int precision, void* workspace,
-                            size_t workspace_bytes, lddmm_stream_t stream);
+int lddmm_apply_diff_k1and2(const double* x, const double* a1, const double* a2, int64_t n, double sigma, int kernel,
+                            const double* origin, double* out, int precision, void* workspace, size_t workspace_bytes,
+                            lddmm_stream_t stream);
 
 /* out(n) = divergence of K(., x) a at y.  Kernel.applyDivergence(x, a, firstVar=y)  base/kernelFunctions.py:638. */
 int lddmm_apply_divergence(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
-                           const double* origin, double* out, int precision, void* workspace,
+                           int kernel, const double* origin, double* out, int precision, void* workspace,
                            size_t workspace_bytes, lddmm_stream_t stream);
 
-/* out(n) = sum_l K(y_k, x_l) (ay_k ax_l + (by_k.bx_l)^2).  Kernel.applyKTensor  base/kernelFunctions.py:509. */
-int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m, const double* ay,
-                         const double* ax, const double* by, const double* bx, double sigma, const double* origin,
-                         double* out, int precision, void* workspace, size_t workspace_bytes,
-                         lddmm_stream_t stream);
+/* out(n) = sum_l K(y_k, x_l) (ay_k ax_l + (by_k.bx_l)^2) with the Gaussian K.  Kernel.applyKTensor
+ * base/kernelFunctions.py:509. */
+int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m, const double* ay, const double* ax,
+                         const double* by, const double* bx, double sigma, const double* origin, double* out,
+                         int precision, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* out(n,3) = K(y, x) a without any workspace argument and without allocating: lddmm_apply_k for callers that
  * cannot allocate device memory at call time (an application whose device-memory budget is fixed at start-up, a
@@ -99,51 +107,50 @@ int lddmm_apply_k_static(const double* y, int64_t n, const double* x, const doub
 /* Dense-weight variants (O(n m) weights streamed from HBM).
  * out(n,d) = sum_l K(y_k, x_l) u[k,l,:]  -- Kernel.applyK(matrixWeights=True) -> ku.applykmat  kernelFunctions_util.py:1509
  * out(n,3) = sum_l -(y_k-x_l)/sigma^2 K beta[k,l] -- Kernel.applyDiffKmat -> ku.applykdiffmat  kernelFunctions_util.py:1631 */
-int lddmm_apply_k_mat(const double* y, int64_t n, const double* x, int64_t m, const double* u, int64_t d,
-                      double sigma, double* out, lddmm_stream_t stream);
-int lddmm_apply_diff_k_mat(const double* y, int64_t n, const double* x, int64_t m, const double* beta,
-                           double sigma, double* out, lddmm_stream_t stream);
+int lddmm_apply_k_mat(const double* y, int64_t n, const double* x, int64_t m, const double* u, int64_t d, double sigma,
+                      double* out, lddmm_stream_t stream);
+int lddmm_apply_diff_k_mat(const double* y, int64_t n, const double* x, int64_t m, const double* beta, double sigma,
+                           double* out, lddmm_stream_t stream);
 
 /* ---------------------------------------------------------------------------------------------------------
  * Landmark shooting and adjoint (replace base/pointEvolution.py). Fused kernels share one exp per pair.
+ * `kernel`: LDDMM_KERNEL_GAUSS or LDDMM_KERNEL_LAPLACIAN(order), as for the kernel operators.
  * ------------------------------------------------------------------------------------------------------- */
 
 /* One second-order (geodesic) Euler step: x1 = x + dt K(x)a, a1 = a - dt DK^T(x; a, a).
  * secondOrderEvolution loop body, base/pointEvolution.py:433-449. */
-int lddmm_second_order_step(const double* x, const double* a, int64_t n, double sigma, double dt,
+int lddmm_second_order_step(const double* x, const double* a, int64_t n, double sigma, int kernel, double dt,
                             const double* origin, double* x_next, double* a_next, int precision, void* workspace,
                             size_t workspace_bytes, lddmm_stream_t stream);
 
 /* Second-order shooting over T steps of size dt: xt, at (T+1,n,3) with xt[0]=x0, at[0]=a0.
  * secondOrderEvolution  base/pointEvolution.py:385. */
-int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int64_t T, double sigma, double dt,
-                             const double* origin, double* xt, double* at, int precision, void* workspace,
+int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int64_t T, double sigma, int kernel,
+                             double dt, const double* origin, double* xt, double* at, int precision, void* workspace,
                              size_t workspace_bytes, lddmm_stream_t stream);
 
 /* One adjoint step (base/pointEvolution.py:539-546):
  * px_prev = px + dt [DK^T_sym(x; px, a) - DDK11and12(x; a, a, pa)],  pa_prev = pa + dt [K(x) px - DK1and2(x; pa, a)]. */
-int lddmm_second_order_adjoint_step(const double* x, const double* a, const double* px, const double* pa,
-                                    int64_t n, double sigma, double dt, const double* origin, double* px_prev,
+int lddmm_second_order_adjoint_step(const double* x, const double* a, const double* px, const double* pa, int64_t n,
+                                    double sigma, int kernel, double dt, const double* origin, double* px_prev,
                                     double* pa_prev, int precision, void* workspace, size_t workspace_bytes,
                                     lddmm_stream_t stream);
 
 /* Row-range forms for sharding one time step over several GPUs (targets = rows row0 .. row0+nrows-1 of the full
  * state, sources = all n rows; outputs are the nrows new rows). Same sums as the whole-step entry points above
  * (base/pointEvolution.py:433-449 and :539-546); workspace: lddmm_workspace_bytes(nrows, n, precision). */
-int lddmm_second_order_step_rows(const double* x, const double* a, int64_t n, int64_t row0, int64_t nrows,
-                                 double sigma, double dt, const double* origin, double* x_next_rows,
-                                 double* a_next_rows, int precision, void* workspace, size_t workspace_bytes,
-                                 lddmm_stream_t stream);
+int lddmm_second_order_step_rows(const double* x, const double* a, int64_t n, int64_t row0, int64_t nrows, double sigma,
+                                 int kernel, double dt, const double* origin, double* x_next_rows, double* a_next_rows,
+                                 int precision, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 int lddmm_second_order_adjoint_step_rows(const double* x, const double* a, const double* px, const double* pa,
-                                         int64_t n, int64_t row0, int64_t nrows, double sigma, double dt,
+                                         int64_t n, int64_t row0, int64_t nrows, double sigma, int kernel, double dt,
                                          const double* origin, double* px_prev_rows, double* pa_prev_rows,
-                                         int precision, void* workspace, size_t workspace_bytes,
-                                         lddmm_stream_t stream);
+                                         int precision, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* Full adjoint sweep + gradient: given xt, at (T+1,n,3) and px1, pa1 (n,3), writes pxt, pat (T+1,n,3) and
  * da0 = K(x0) a0 - pat[0].  secondOrderCovector / secondOrderGradient  base/pointEvolution.py:489-618. */
-int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, double dt,
-                                const double* px1, const double* pa1, const double* origin, double* pxt,
+int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, int kernel,
+                                double dt, const double* px1, const double* pa1, const double* origin, double* pxt,
                                 double* pat, double* da0, int precision, void* workspace, size_t workspace_bytes,
                                 lddmm_stream_t stream);
 
@@ -151,7 +158,7 @@ int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, i
  * energy[0] = regweight * dt * sum_t a_t . K(x_t) a_t (device scalar, FP64, deterministic order).
  * landmarkDirectEvolutionEuler base/pointEvolution.py:88 + SurfaceMatching.objectiveFunDef base/surfaceMatching.py:546.
  * `energy` may be NULL. */
-int lddmm_first_order_shoot(const double* x0, const double* at, int64_t n, int64_t T, double sigma,
+int lddmm_first_order_shoot(const double* x0, const double* at, int64_t n, int64_t T, double sigma, int kernel,
                             double regweight, const double* origin, double* xt, double* energy, int precision,
                             void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
@@ -160,7 +167,7 @@ int lddmm_first_order_shoot(const double* x0, const double* at, int64_t n, int64
  *   dat_t = 2 regweight a_t - p_{t+1}            (euclidean = 0)
  *   dat_t = K(x_t)(2 regweight a_t - p_{t+1})    (euclidean = 1, the BFGS gradient of SurfaceMatching).
  * Both sums of a step share one exp per pair. pxt (T+1,n,3), dat (T,n,3). */
-int lddmm_first_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma,
+int lddmm_first_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, int kernel,
                                double regweight, const double* px1, int euclidean, const double* origin, double* pxt,
                                double* dat, int precision, void* workspace, size_t workspace_bytes,
                                lddmm_stream_t stream);
@@ -179,9 +186,8 @@ size_t lddmm_surface_workspace_bytes(int64_t nf, int64_t nf1, int precision);
  * varifoldNormDef / varifoldNorm0  base/surfaceDistances.py:286-382 (current :22-81, measure :207-223). */
 int lddmm_surface_energy(int kind, const double* xdef, int64_t nv, const int64_t* faces, int64_t nf,
                          const double* weights, const double* x1, int64_t nv1, const int64_t* faces1, int64_t nf1,
-                         const double* weights1, double sigma, const double* origin, int with_norm0,
-                         double* energy, int precision, void* workspace, size_t workspace_bytes,
-                         lddmm_stream_t stream);
+                         const double* weights1, double sigma, const double* origin, int with_norm0, double* energy,
+                         int precision, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
 
 /* Vertex gradient of xNormDef: px (nv,3) and, for the varifold when pxw != NULL, the vertex-weight gradient
  * pxw (nv) (varifoldNormGradient(with_weights=True)). The faces->vertices scatter is a deterministic gather
@@ -189,10 +195,10 @@ int lddmm_surface_energy(int kind, const double* xdef, int64_t nv, const int64_t
  * 3*face + corner), built once per topology by lddmm_vertex_face_table.
  * varifoldNormGradient base/surfaceDistances.py:394-573 (current :90-133, measure :232-278). */
 int lddmm_surface_gradient(int kind, const double* xdef, int64_t nv, const int64_t* faces, int64_t nf,
-                           const double* weights, const int32_t* vf_offsets, const int32_t* vf_items,
-                           const double* x1, int64_t nv1, const int64_t* faces1, int64_t nf1,
-                           const double* weights1, double sigma, const double* origin, double* px, double* pxw,
-                           int precision, void* workspace, size_t workspace_bytes, lddmm_stream_t stream);
+                           const double* weights, const int32_t* vf_offsets, const int32_t* vf_items, const double* x1,
+                           int64_t nv1, const int64_t* faces1, int64_t nf1, const double* weights1, double sigma,
+                           const double* origin, double* px, double* pxw, int precision, void* workspace,
+                           size_t workspace_bytes, lddmm_stream_t stream);
 
 /* Host-side helper (HOST pointers): vertex -> (face, corner) incidence table in ascending (face, corner) order. */
 int lddmm_vertex_face_table(const int64_t* faces_host, int64_t nf, int64_t nv, int32_t* vf_offsets_host,

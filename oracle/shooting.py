@@ -1,39 +1,46 @@
 """Float64 CPU restatement of landmark shooting and its adjoint (no affine part, no splines).
 
-Reference: base/pointEvolution.py. TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
+Reference: base/pointEvolution.py. Every function takes `ops`, the kernel operator set: the Gaussian one of
+oracle/kernels.py by default, or oracle.laplacian.ops(order). TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 """
+import types
+
 import numpy as np
 
-from .kernels import apply_k, apply_diff_kt, apply_ddiff_k11and12, apply_diff_k1and2
+from . import kernels as _gauss
+
+GAUSS = types.SimpleNamespace(apply_k=_gauss.apply_k, apply_diff_kt=_gauss.apply_diff_kt,
+                              apply_ddiff_k11and12=_gauss.apply_ddiff_k11and12,
+                              apply_diff_k1and2=_gauss.apply_diff_k1and2)
 
 
-def landmark_direct_evolution_euler(x0, at, sigma):
+def landmark_direct_evolution_euler(x0, at, sigma, ops=GAUSS):
     """x_{t+1} = x_t + dt K(x_t) a_t, dt = 1/T  (base/pointEvolution.py:88-164)."""
     T = at.shape[0]
     dt = 1.0 / T
     xt = np.zeros((T + 1,) + x0.shape)
     xt[0] = x0
     for t in range(T):
-        xt[t + 1] = xt[t] + dt * apply_k(xt[t], xt[t], at[t], sigma)
+        xt[t + 1] = xt[t] + dt * ops.apply_k(xt[t], xt[t], at[t], sigma)
     return xt
 
 
-def landmark_hamiltonian_gradient(x0, at, px1, sigma, regweight):
+def landmark_hamiltonian_gradient(x0, at, px1, sigma, regweight, ops=GAUSS):
     """Backward sweep p_t = p_{t+1} + dt DK^T_lddmm(x_t; p_{t+1}, a_t); dat_t = 2 w a_t - p_{t+1}
     (base/pointEvolution.py:167-236). Returns (dat, xt, pxt)."""
     T = at.shape[0]
     dt = 1.0 / T
-    xt = landmark_direct_evolution_euler(x0, at, sigma)
+    xt = landmark_direct_evolution_euler(x0, at, sigma, ops)
     pxt = np.zeros((T + 1,) + x0.shape)
     pxt[T] = px1
     for t in range(T - 1, -1, -1):
         px = pxt[t + 1]
-        pxt[t] = px + dt * apply_diff_kt(xt[t], xt[t], px, at[t], sigma, lddmm=True, regweight=regweight)
+        pxt[t] = px + dt * ops.apply_diff_kt(xt[t], xt[t], px, at[t], sigma, lddmm=True, regweight=regweight)
     dat = 2.0 * regweight * at - pxt[1:]
     return dat, xt, pxt
 
 
-def second_order_evolution(x0, a0, sigma, timeStep):
+def second_order_evolution(x0, a0, sigma, timeStep, ops=GAUSS):
     """x += dt K(x) a, a -= dt DK^T(x; a, a), T = round(1/timeStep) steps of size timeStep
     (base/pointEvolution.py:385-472). Returns (xt, at)."""
     T = int(np.round(1.0 / timeStep))
@@ -42,27 +49,27 @@ def second_order_evolution(x0, a0, sigma, timeStep):
     xt[0], at[0] = x0, a0
     for k in range(T):
         x, a = xt[k], at[k]
-        zx = apply_k(x, x, a, sigma)
-        za = -apply_diff_kt(x, x, a, a, sigma)
+        zx = ops.apply_k(x, x, a, sigma)
+        za = -ops.apply_diff_kt(x, x, a, a, sigma)
         xt[k + 1] = x + timeStep * zx
         at[k + 1] = a + timeStep * za
     return xt, at
 
 
-def second_order_gradient(x0, a0, px1, pa1, sigma, timeStep):
+def second_order_gradient(x0, a0, px1, pa1, sigma, timeStep, ops=GAUSS):
     """Adjoint of second-order shooting (base/pointEvolution.py:489-618):
     px <- px + dt [DK^T_sym(x; px, a) - DDK11and12(x; a, a, pa)], pa <- pa + dt [K(x) px - DK1and2(x; pa, a)],
     da0 = K(x0) a0 - pa_0. Returns dict(da0, xt, at, pxt, pat)."""
     T = int(np.round(1.0 / timeStep))
-    xt, at = second_order_evolution(x0, a0, sigma, timeStep)
+    xt, at = second_order_evolution(x0, a0, sigma, timeStep, ops)
     pxt = np.zeros((T + 1,) + x0.shape)
     pat = np.zeros((T + 1,) + x0.shape)
     pxt[T], pat[T] = px1, pa1
     for t in range(T - 1, -1, -1):
         px, pa, x, a = pxt[t + 1], pat[t + 1], xt[t], at[t]
-        zpx = apply_diff_kt(x, x, px, a, sigma, sym=True) - apply_ddiff_k11and12(x, a, a, pa, sigma)
-        zpa = apply_k(x, x, px, sigma) - apply_diff_k1and2(x, pa, a, sigma)
+        zpx = ops.apply_diff_kt(x, x, px, a, sigma, sym=True) - ops.apply_ddiff_k11and12(x, a, a, pa, sigma)
+        zpa = ops.apply_k(x, x, px, sigma) - ops.apply_diff_k1and2(x, pa, a, sigma)
         pxt[t] = px + timeStep * zpx
         pat[t] = pa + timeStep * zpa
-    da0 = apply_k(x0, x0, a0, sigma) - pat[0]
+    da0 = ops.apply_k(x0, x0, a0, sigma) - pat[0]
     return dict(da0=da0, xt=xt, at=at, pxt=pxt, pat=pat)

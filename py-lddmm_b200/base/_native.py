@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), 'lib', 'liblddmm_b200.so')
 
 FP32C = 0
 FP64 = 1
+KERNEL_GAUSS = 0
+KERNEL_LAPLACIAN0 = 16     # + order (0..4)
 DATA_VARIFOLD, DATA_CURRENT, DATA_MEASURE = 0, 1, 2
 
 _i64, _f64, _int, _sz, _vp = ctypes.c_int64, ctypes.c_double, ctypes.c_int, ctypes.c_size_t, ctypes.c_void_p
@@ -27,25 +29,28 @@ SIGNATURES = {
     'lddmm_status_string': [_int],
     'lddmm_workspace_bytes': [_i64, _i64, _int],
     'lddmm_surface_workspace_bytes': [_i64, _i64, _int],
-    'lddmm_apply_k': [_dp, _i64, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_apply_diff_kt': [_dp, _i64, _dp, _dp, _dp, _i64, _f64, _int, _f64, _hp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_apply_ddiff_k11and12': [_dp, _dp, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_apply_diff_k1and2': [_dp, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_apply_divergence': [_dp, _i64, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_apply_k': [_dp, _i64, _dp, _dp, _i64, _f64, _int, _hp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_apply_diff_kt': [_dp, _i64, _dp, _dp, _dp, _i64, _f64, _int, _int, _f64, _hp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_apply_ddiff_k11and12': [_dp, _dp, _dp, _dp, _i64, _f64, _int, _hp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_apply_diff_k1and2': [_dp, _dp, _dp, _i64, _f64, _int, _hp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_apply_divergence': [_dp, _i64, _dp, _dp, _i64, _f64, _int, _hp, _dp, _int, _vp, _sz, _vp],
     'lddmm_apply_k_tensor': [_dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _f64, _hp, _dp, _int, _vp, _sz, _vp],
     'lddmm_apply_k_static': [_dp, _i64, _dp, _dp, _i64, _f64, _hp, _dp, _int, _vp],
     'lddmm_apply_k_mat': [_dp, _i64, _dp, _i64, _dp, _i64, _f64, _dp, _vp],
     'lddmm_apply_diff_k_mat': [_dp, _i64, _dp, _i64, _dp, _f64, _dp, _vp],
-    'lddmm_second_order_step': [_dp, _dp, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_second_order_shoot': [_dp, _dp, _i64, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_second_order_step_rows': [_dp, _dp, _i64, _i64, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_second_order_adjoint_step_rows': [_dp, _dp, _dp, _dp, _i64, _i64, _i64, _f64, _f64, _hp, _dp, _dp,
+    'lddmm_second_order_step': [_dp, _dp, _i64, _f64, _int, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_second_order_shoot': [_dp, _dp, _i64, _i64, _f64, _int, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_second_order_step_rows': [_dp, _dp, _i64, _i64, _i64, _f64, _int, _f64, _hp, _dp, _dp, _int, _vp, _sz,
+                                     _vp],
+    'lddmm_second_order_adjoint_step_rows': [_dp, _dp, _dp, _dp, _i64, _i64, _i64, _f64, _int, _f64, _hp, _dp, _dp,
                                              _int, _vp, _sz, _vp],
-    'lddmm_second_order_adjoint_step': [_dp, _dp, _dp, _dp, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_second_order_gradient': [_dp, _dp, _i64, _i64, _f64, _f64, _dp, _dp, _hp, _dp, _dp, _dp, _int, _vp, _sz,
-                                    _vp],
-    'lddmm_first_order_shoot': [_dp, _dp, _i64, _i64, _f64, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
-    'lddmm_first_order_gradient': [_dp, _dp, _i64, _i64, _f64, _f64, _dp, _int, _hp, _dp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_second_order_adjoint_step': [_dp, _dp, _dp, _dp, _i64, _f64, _int, _f64, _hp, _dp, _dp, _int, _vp, _sz,
+                                        _vp],
+    'lddmm_second_order_gradient': [_dp, _dp, _i64, _i64, _f64, _int, _f64, _dp, _dp, _hp, _dp, _dp, _dp, _int, _vp,
+                                    _sz, _vp],
+    'lddmm_first_order_shoot': [_dp, _dp, _i64, _i64, _f64, _int, _f64, _hp, _dp, _dp, _int, _vp, _sz, _vp],
+    'lddmm_first_order_gradient': [_dp, _dp, _i64, _i64, _f64, _int, _f64, _dp, _int, _hp, _dp, _dp, _int, _vp, _sz,
+                                   _vp],
     'lddmm_surface_energy': [_int, _dp, _i64, _dp, _i64, _dp, _dp, _i64, _dp, _i64, _dp, _f64, _hp, _int, _dp, _int,
                              _vp, _sz, _vp],
     'lddmm_surface_gradient': [_int, _dp, _i64, _dp, _i64, _dp, _dp, _dp, _dp, _i64, _dp, _i64, _dp, _f64, _hp, _dp,
@@ -91,6 +96,16 @@ def lib():
                     raise LddmmError('lddmm_b200 needs a CUDA device (sm_100a); none is available')
                 _lib = load_library()
     return _lib
+
+
+def kernel_code(K):
+    """The library's kernel-family argument for a Kernel: 0 (Gaussian) or 16 + order ('laplacian')."""
+    name = getattr(K, 'name', 'gauss')
+    if name in ('gauss', 'gaussian'):
+        return KERNEL_GAUSS
+    if name == 'laplacian':
+        return KERNEL_LAPLACIAN0 + int(K.order)
+    raise NotImplementedError(f"lddmm_b200 implements the 'gauss' and 'laplacian' kernels (got '{name}')")
 
 
 def check(status, what=''):

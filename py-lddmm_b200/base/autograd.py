@@ -31,8 +31,8 @@ def _sigma(K):
 
 def _step_forward(K, x, a, dt, origin, ws):
     x1, a1 = torch.empty_like(x), torch.empty_like(a)
-    nat.check(nat.lib().lddmm_second_order_step(nat.ptr(x), nat.ptr(a), x.shape[0], _sigma(K), float(dt), origin,
-                                                nat.ptr(x1), nat.ptr(a1), K.precision, ws[0], ws[1],
+    nat.check(nat.lib().lddmm_second_order_step(nat.ptr(x), nat.ptr(a), x.shape[0], _sigma(K), K.code, float(dt),
+                                                origin, nat.ptr(x1), nat.ptr(a1), K.precision, ws[0], ws[1],
                                                 nat.stream_ptr()), 'second_order_step')
     return x1, a1
 
@@ -40,8 +40,8 @@ def _step_forward(K, x, a, dt, origin, ws):
 def _step_adjoint(K, x, a, px, pa, dt, origin, ws):
     px0, pa0 = torch.empty_like(px), torch.empty_like(pa)
     nat.check(nat.lib().lddmm_second_order_adjoint_step(nat.ptr(x), nat.ptr(a), nat.ptr(px), nat.ptr(pa), x.shape[0],
-                                                        _sigma(K), float(dt), origin, nat.ptr(px0), nat.ptr(pa0),
-                                                        K.precision, ws[0], ws[1], nat.stream_ptr()),
+                                                        _sigma(K), K.code, float(dt), origin, nat.ptr(px0),
+                                                        nat.ptr(pa0), K.precision, ws[0], ws[1], nat.stream_ptr()),
               'second_order_adjoint_step')
     return px0, pa0
 

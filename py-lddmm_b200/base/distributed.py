@@ -46,8 +46,8 @@ def library_step_rows(K, origin):
         x1 = torch.empty((nr, 3), dtype=torch.float64, device=x.device)
         a1 = torch.empty_like(x1)
         ws, wsb = nat.workspace(max(nr, 1), n, K.precision)
-        nat.check(nat.lib().lddmm_second_order_step_rows(nat.ptr(x), nat.ptr(a), n, r0, nr, sigma, float(dt), o,
-                                                         nat.ptr(x1), nat.ptr(a1), K.precision, ws, wsb,
+        nat.check(nat.lib().lddmm_second_order_step_rows(nat.ptr(x), nat.ptr(a), n, r0, nr, sigma, K.code, float(dt),
+                                                         o, nat.ptr(x1), nat.ptr(a1), K.precision, ws, wsb,
                                                          nat.stream_ptr()), 'second_order_step_rows')
         return x1, a1
     return step
@@ -64,8 +64,8 @@ def library_adjoint_rows(K, origin):
         q0 = torch.empty_like(p0)
         ws, wsb = nat.workspace(max(nr, 1), n, K.precision)
         nat.check(nat.lib().lddmm_second_order_adjoint_step_rows(nat.ptr(x), nat.ptr(a), nat.ptr(px), nat.ptr(pa), n,
-                                                                 r0, nr, sigma, float(dt), o, nat.ptr(p0), nat.ptr(q0),
-                                                                 K.precision, ws, wsb, nat.stream_ptr()),
+                                                                 r0, nr, sigma, K.code, float(dt), o, nat.ptr(p0),
+                                                                 nat.ptr(q0), K.precision, ws, wsb, nat.stream_ptr()),
                   'second_order_adjoint_step_rows')
         return p0, q0
     return step

@@ -4,8 +4,11 @@ Signatures, argument meaning and return shapes follow the reference. Inputs may 
 reference's contract: numpy in, new numpy array out, inputs never written) or torch tensors (CUDA or CPU);
 the result has the type of `x`. Every sum runs in the CUDA library (no CPU fallback).
 
-Supported: the Gaussian kernel ('gauss' / 'gaussian') with one or several widths (multi-scale sums weighted
-by sigma**ms_exponent / sum(sigma**ms_exponent), base/kernelFunctions_util.py:451-466), affine='none'.
+Supported: the Gaussian kernel ('gauss' / 'gaussian') and the reference's Laplacian (Matern) kernel
+('laplacian', order 0..4: P_order(r/sigma) exp(-r/sigma), base/kernelFunctions_util.py:20-56), with one or several
+widths (multi-scale sums weighted by sigma**ms_exponent / sum(sigma**ms_exponent),
+base/kernelFunctions_util.py:451-466), affine='none'. applyKTensor and the dense-weight variants (matrixWeights,
+applyDiffKmat) are Gaussian only, as are the surface data terms.
 `pk_dtype` selects the arithmetic: 'float32' -> FP32 pair sums with compensated accumulation,
 'float64' -> FP64 pair sums (the faithful path); both return float64 like the reference.
 """
@@ -17,6 +20,10 @@ import torch
 from . import _native as nat
 
 _GAUSS = ('gauss', 'gaussian')
+_FAMILIES = _GAUSS + ('laplacian',)
+# lapPol coefficients of the Laplacian kernel by order (base/kernelFunctions_util.py:20-24)
+_LAP_POLY = ((1, 0, 0, 0, 0), (1, 1, 0, 0, 0), (1, 1, 1 / 3, 0, 0), (1, 1, 0.4, 1 / 15, 0),
+             (1, 1, 3 / 7, 2 / 21, 1 / 105))
 
 
 def _is_np(v):
@@ -43,10 +50,14 @@ class KernelSpec:
         self._state = False
         self.localMaps = localMaps
         self.setAffine(affine, w1, w2)
-        self.kff = name in _GAUSS
+        self.kff = name in _FAMILIES
         self.pk_dtype = 'float64'
         self.ms_exponent = -1
-        if name in _GAUSS:
+        if name == 'laplacian':
+            if self.order > 4:
+                self.order = 3
+            self.par = [sigma, self.order]
+        elif name in _GAUSS:
             self.order = 10
             self.par = [sigma]
         else:
@@ -63,13 +74,19 @@ class Kernel(KernelSpec):
     """Gaussian kernel operators on the B200 (base/kernelFunctions.py:414-680)."""
 
     # ------------------------------------------------------------------ helpers
-    def _check(self):
-        if self.name not in _GAUSS:
-            raise NotImplementedError(f"lddmm_b200 implements the Gaussian kernel only (got '{self.name}')")
+    def _check(self, gauss_only=False):
+        if self.name not in (_GAUSS if gauss_only else _FAMILIES):
+            what = 'the Gaussian kernel' if gauss_only else "the 'gauss' and 'laplacian' kernels"
+            raise NotImplementedError(f"lddmm_b200 implements {what} here (got '{self.name}')")
         if self.affine not in (None, 'none'):
             raise NotImplementedError("lddmm_b200 implements affine='none' only")
         if self.localMaps:
             raise NotImplementedError('lddmm_b200 does not implement localMaps kernels')
+
+    @property
+    def code(self):
+        """Kernel-family argument of the library (0: Gaussian, 16 + order: Laplacian)."""
+        return nat.kernel_code(self)
 
     @property
     def precision(self):
@@ -96,6 +113,7 @@ class Kernel(KernelSpec):
         X = nat.as_device(x)
         Y = X if firstVar is None else nat.as_device(firstVar)
         if matrixWeights:
+            self._check(gauss_only=True)
             U = nat.as_device(a)
             if U.dim() == 2:
                 U = U[..., None]
@@ -119,8 +137,8 @@ class Kernel(KernelSpec):
         out = torch.empty((n, 3), dtype=torch.float64, device=Y.device)
         ws, wsb = nat.workspace(n, m, self.precision)
         o = nat.origin_arg(origin if origin is not None else nat.centroid(X))
-        nat.check(nat.lib().lddmm_apply_k(nat.ptr(Y), n, nat.ptr(X), nat.ptr(A), m, float(sigma), o, nat.ptr(out),
-                                          self.precision, ws, wsb, nat.stream_ptr()), 'applyK')
+        nat.check(nat.lib().lddmm_apply_k(nat.ptr(Y), n, nat.ptr(X), nat.ptr(A), m, float(sigma), self.code, o,
+                                          nat.ptr(out), self.precision, ws, wsb, nat.stream_ptr()), 'applyK')
         return out
 
     def _k_generic(self, Y, X, A, sigma, origin=None):
@@ -143,7 +161,7 @@ class Kernel(KernelSpec):
 
     def applyKTensor(self, x, ay, ax, betay, betax, firstVar=None, grid=None, cpu=False):
         """sum_l K_kl (ay_k ax_l + (betay_k.betax_l)^2) (base/kernelFunctions.py:509-517)."""
-        self._check()
+        self._check(gauss_only=True)
         like_np = _is_np(x)
         X = nat.as_device(x)
         Y = X if firstVar is None else nat.as_device(firstVar)
@@ -168,8 +186,8 @@ class Kernel(KernelSpec):
         out = torch.empty((n, 3), dtype=torch.float64, device=X.device)
         ws, wsb = nat.workspace(n, n, self.precision)
         o = nat.origin_arg(nat.centroid(X))
-        nat.check(nat.lib().lddmm_apply_diff_k1and2(nat.ptr(X), nat.ptr(A1), nat.ptr(A2), n, float(sigma), o,
-                                                    nat.ptr(out), self.precision, ws, wsb, nat.stream_ptr()),
+        nat.check(nat.lib().lddmm_apply_diff_k1and2(nat.ptr(X), nat.ptr(A1), nat.ptr(A2), n, float(sigma), self.code,
+                                                    o, nat.ptr(out), self.precision, ws, wsb, nat.stream_ptr()),
                   'applyDiffK1and2')
         return out
 
@@ -207,7 +225,7 @@ class Kernel(KernelSpec):
 
     def applyDiffKmat(self, x, beta, firstVar=None):
         """sum_l -(y_k - x_l)/sigma^2 K_kl beta[k,l] (base/kernelFunctions.py:565-570)."""
-        self._check()
+        self._check(gauss_only=True)
         like_np = _is_np(x)
         X = nat.as_device(x)
         Y = X if firstVar is None else nat.as_device(firstVar)
@@ -260,8 +278,8 @@ class Kernel(KernelSpec):
             out = torch.empty((n, 3), dtype=torch.float64, device=Y.device)
             ws, wsb = nat.workspace(n, m, self.precision)
             nat.check(nat.lib().lddmm_apply_diff_kt(nat.ptr(Y), n, nat.ptr(X), nat.ptr(P), nat.ptr(A), m, float(s),
-                                                    mode, float(regweight), o, nat.ptr(out), self.precision, ws, wsb,
-                                                    nat.stream_ptr()), 'applyDiffKT')
+                                                    self.code, mode, float(regweight), o, nat.ptr(out),
+                                                    self.precision, ws, wsb, nat.stream_ptr()), 'applyDiffKT')
             return out
         return self._multi(one)
 
@@ -289,8 +307,8 @@ class Kernel(KernelSpec):
         def one(s):
             out = torch.empty((n, 1), dtype=torch.float64, device=Y.device)
             ws, wsb = nat.workspace(n, m, self.precision)
-            nat.check(nat.lib().lddmm_apply_divergence(nat.ptr(Y), n, nat.ptr(X), nat.ptr(A), m, float(s), o,
-                                                       nat.ptr(out), self.precision, ws, wsb, nat.stream_ptr()),
+            nat.check(nat.lib().lddmm_apply_divergence(nat.ptr(Y), n, nat.ptr(X), nat.ptr(A), m, float(s), self.code,
+                                                       o, nat.ptr(out), self.precision, ws, wsb, nat.stream_ptr()),
                       'applyDivergence')
             return out
         return _out(self._multi(one), like_np)
@@ -308,8 +326,8 @@ class Kernel(KernelSpec):
             out = torch.empty((N, 3), dtype=torch.float64, device=X.device)
             ws, wsb = nat.workspace(N, N, self.precision)
             nat.check(nat.lib().lddmm_apply_ddiff_k11and12(nat.ptr(X), nat.ptr(Nn), nat.ptr(A), nat.ptr(P), N,
-                                                           float(s), o, nat.ptr(out), self.precision, ws, wsb,
-                                                           nat.stream_ptr()), 'applyDDiffK11and12')
+                                                           float(s), self.code, o, nat.ptr(out), self.precision, ws,
+                                                           wsb, nat.stream_ptr()), 'applyDDiffK11and12')
             return out
         return _out(self._multi(one), like_np)
 
@@ -321,7 +339,16 @@ class Kernel(KernelSpec):
         X = nat.as_device(x)
         Y = X if firstVar is None else nat.as_device(firstVar)
         d2 = ((Y[:, None, :] - X[None, :, :]) ** 2).sum(-1)
-        K = self._multi(lambda s: torch.exp(-d2 / (2 * s * s)))
+        if self.name == 'laplacian':
+            c = _LAP_POLY[int(self.order)]
+            r = torch.sqrt(d2)
+
+            def lap(s):
+                u = r / s
+                return (c[0] + u * (c[1] + u * (c[2] + u * (c[3] + u * c[4])))) * torch.exp(-u)
+            K = self._multi(lap)
+        else:
+            K = self._multi(lambda s: torch.exp(-d2 / (2 * s * s)))
         return _out(K, like_np)
 
     def hold(self):

@@ -281,9 +281,11 @@ def train(model, feats, labels, n, epochs=10, batch_pairs=16, lr=1e-3, seed=0, l
     return history
 
 
-def warm_start(matching, model, cg_iters=0):
+def warm_start(matching, model, cg_iters=0, scales=(1.0,)):
     """Set matching.control['a0'] to the network's proposal when it lowers the objective, else keep zero momentum
-    (the plain optimiser is the fallback). Returns (used_proposal, objective_at_proposal, objective_at_zero)."""
+    (the plain optimiser is the fallback). With several `scales`, the proposal is tried at each multiple and the
+    best one is kept (one forward shot per scale). Returns (used_proposal, objective_at_proposal, objective_at_zero,
+    chosen_scale)."""
     X0 = matching.x0
     faces_t = matching.data.faces
     a_prop = model.predict(X0, faces_t, matching.data.x1, matching.options['KparDiff'], cg_iters=cg_iters)
@@ -294,8 +296,16 @@ def warm_start(matching, model, cg_iters=0):
         matching.control['a0'] = zero
         matching.obj = None
         obj_zero = matching.objectiveFun()
-    obj_prop = matching.updateTry({'a0': -a_prop}, 1.0)     # control - 1.0 * (-a_prop) = a_prop
-    used = bool(np.isfinite(obj_prop) and obj_prop < obj_zero)
+    best, best_scale = obj_zero, None
+    obj_prop = None
+    for s in scales:
+        # control - s * (-a_prop) = s * a_prop; updateTry keeps the trial only when it beats `best`
+        o = matching.updateTry({'a0': -a_prop}, float(s), best)
+        if obj_prop is None or (np.isfinite(o) and o < obj_prop):
+            obj_prop = o
+        if np.isfinite(o) and o < best:
+            best, best_scale = o, float(s)
+    used = best_scale is not None
     if used:
         matching.acceptVarTry()
-    return used, obj_prop, obj_zero
+    return used, obj_prop, obj_zero, best_scale

@@ -49,8 +49,8 @@ def shoot_first_order(X0, AT, K, regweight=1.0, energy=None, origin=None):
         return xt
     ws, wsb = nat.workspace(N, N, K.precision)
     o = nat.origin_arg(origin if origin is not None else nat.centroid(X0))
-    nat.check(nat.lib().lddmm_first_order_shoot(nat.ptr(X0), nat.ptr(AT), N, T, sig, float(regweight), o, nat.ptr(xt),
-                                                nat.ptr(energy), K.precision, ws, wsb, nat.stream_ptr()),
+    nat.check(nat.lib().lddmm_first_order_shoot(nat.ptr(X0), nat.ptr(AT), N, T, sig, K.code, float(regweight), o,
+                                                nat.ptr(xt), nat.ptr(energy), K.precision, ws, wsb, nat.stream_ptr()),
               'first_order_shoot')
     return xt
 
@@ -71,7 +71,7 @@ def first_order_gradient(XT, AT, PX1, K, regweight, euclidean=False, origin=None
         return pxt, dat
     ws, wsb = nat.workspace(N, N, K.precision)
     o = nat.origin_arg(origin if origin is not None else nat.centroid(XT[0]))
-    nat.check(nat.lib().lddmm_first_order_gradient(nat.ptr(XT), nat.ptr(AT), N, T, sig, float(regweight),
+    nat.check(nat.lib().lddmm_first_order_gradient(nat.ptr(XT), nat.ptr(AT), N, T, sig, K.code, float(regweight),
                                                    nat.ptr(PX1.contiguous()), int(bool(euclidean)), o, nat.ptr(pxt),
                                                    nat.ptr(dat), K.precision, ws, wsb, nat.stream_ptr()),
               'first_order_gradient')
@@ -93,8 +93,8 @@ def shoot_second_order(X0, A0, K, timeStep, origin=None):
         return xt, at
     ws, wsb = nat.workspace(N, N, K.precision)
     o = nat.origin_arg(origin if origin is not None else nat.centroid(X0))
-    nat.check(nat.lib().lddmm_second_order_shoot(nat.ptr(X0), nat.ptr(A0), N, T, sig, float(timeStep), o, nat.ptr(xt),
-                                                 nat.ptr(at), K.precision, ws, wsb, nat.stream_ptr()),
+    nat.check(nat.lib().lddmm_second_order_shoot(nat.ptr(X0), nat.ptr(A0), N, T, sig, K.code, float(timeStep), o,
+                                                 nat.ptr(xt), nat.ptr(at), K.precision, ws, wsb, nat.stream_ptr()),
               'second_order_shoot')
     return xt, at
 
@@ -120,7 +120,7 @@ def second_order_adjoint(XT, AT, PX1, PA1, K, timeStep, origin=None, with_da0=Tr
         return pxt, pat, da0
     ws, wsb = nat.workspace(N, N, K.precision)
     o = nat.origin_arg(origin if origin is not None else nat.centroid(XT[0]))
-    nat.check(nat.lib().lddmm_second_order_gradient(nat.ptr(XT), nat.ptr(AT), N, T, sig, float(timeStep),
+    nat.check(nat.lib().lddmm_second_order_gradient(nat.ptr(XT), nat.ptr(AT), N, T, sig, K.code, float(timeStep),
                                                     nat.ptr(PX1.contiguous()), nat.ptr(PA1.contiguous()), o,
                                                     nat.ptr(pxt), nat.ptr(pat), nat.ptr(da0), K.precision, ws, wsb,
                                                     nat.stream_ptr()), 'second_order_gradient')

@@ -44,13 +44,13 @@ struct OpK {
     src_point(P.x, l, P.f, f);
     f[3] = P.a[3 * l]; f[4] = P.a[3 * l + 1]; f[5] = P.a[3 * l + 2];
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
-    acc[0] = fma(e, s[3], acc[0]);
-    acc[1] = fma(e, s[4], acc[1]);
-    acc[2] = fma(e, s[5], acc[2]);
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
+    acc[0] = fma(k.k0, s[3], acc[0]);
+    acc[1] = fma(k.k0, s[4], acc[1]);
+    acc[2] = fma(k.k0, s[5], acc[2]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     if (P.dots)
@@ -103,13 +103,13 @@ struct OpDiffKT {
       for (int c = 0; c < 3; ++c) f[6 + c] = P.p[3 * l + c] - k * P.a[3 * l + c];
     }
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
     V c = dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]);
     if (MODE != 0) c = fma(t.a0, s[6], fma(t.a1, s[7], fma(t.a2, s[8], c)));
-    const V ec = e * c;
+    const V ec = k.k1 * c;
     acc[0] = fma(ec, d0, acc[0]);
     acc[1] = fma(ec, d1, acc[1]);
     acc[2] = fma(ec, d2, acc[2]);
@@ -153,13 +153,14 @@ struct OpDDiffK {
       f[6 + c] = P.p[3 * l + c];
     }
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
     const V dq = dot3(d0, d1, d2, t.p0 - s[6], t.p1 - s[7], t.p2 - s[8]);
-    const V ce = e * dot3(t.n0, t.n1, t.n2, s[3], s[4], s[5]);
-    const V ced = ce * dq;
+    const V na = dot3(t.n0, t.n1, t.n2, s[3], s[4], s[5]);
+    const V ce = k.k1 * na;
+    const V ced = (k.k2 * na) * dq;  // == ce * dq for the Gaussian
     acc[0] = fma(ced, d0, acc[0]);
     acc[1] = fma(ced, d1, acc[1]);
     acc[2] = fma(ced, d2, acc[2]);
@@ -201,11 +202,11 @@ struct OpDiffK1and2 {
       f[6 + c] = P.a2[3 * l + c];
     }
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
-    const V eg = e * dot3(d0, d1, d2, t.b0 - s[3], t.b1 - s[4], t.b2 - s[5]);
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
+    const V eg = k.k1 * dot3(d0, d1, d2, t.b0 - s[3], t.b1 - s[4], t.b2 - s[5]);
     acc[0] = fma(eg, s[6], acc[0]);
     acc[1] = fma(eg, s[7], acc[1]);
     acc[2] = fma(eg, s[8], acc[2]);
@@ -238,11 +239,11 @@ struct OpDiv {
     src_point(P.x, l, P.f, f);
     f[3] = P.a[3 * l]; f[4] = P.a[3 * l + 1]; f[5] = P.a[3 * l + 2];
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
-    acc[0] = fma(e, dot3(d0, d1, d2, s[3], s[4], s[5]), acc[0]);
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
+    acc[0] = fma(k.k1, dot3(d0, d1, d2, s[3], s[4], s[5]), acc[0]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     P.out[i] = -P.f.kappa * acc[0];
@@ -273,13 +274,13 @@ struct OpKTensor {
     f[3] = P.ax[l];
     f[4] = P.bx[3 * l]; f[5] = P.bx[3 * l + 1]; f[6] = P.bx[3 * l + 2];
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
     const V g = dot3(t.b0, t.b1, t.b2, s[4], s[5], s[6]);
-    acc[0] = fma(e, s[3], acc[0]);
-    acc[1] = fma(e, g * g, acc[1]);
+    acc[0] = fma(k.k0, s[3], acc[0]);
+    acc[1] = fma(k.k0, g * g, acc[1]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     P.out[i] = P.ay[i] * acc[0] + acc[1];

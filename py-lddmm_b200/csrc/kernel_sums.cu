@@ -1,4 +1,4 @@
-// C-ABI entry points of the Gaussian kernel operators (Kernel.applyK / applyDiffKT / applyDDiffK11and12 /
+// C-ABI entry points of the kernel operators (Kernel.applyK / applyDiffKT / applyDDiffK11and12 /
 // applyDiffK1and2 / applyDivergence / applyKTensor).
 #include "../../include/lddmm_b200.h"
 #include "kernel_ops.cuh"
@@ -47,25 +47,26 @@ namespace {
 bool bad_ptr(const void* p, int64_t count) { return count > 0 && p == nullptr; }
 
 template <class Op, int TPB32, int RT32, class Fill>
-int dispatch(int precision, int64_t n, int64_t m, double sigma, const double* origin, void* ws, size_t wsb,
-             cudaStream_t st, Fill fill) {
+int dispatch(int precision, int64_t n, int64_t m, double sigma, int kernel, const double* origin, void* ws,
+             size_t wsb, cudaStream_t st, Fill fill) {
+  if (bad_kernel(kernel)) return kInvalidArgument;
   typename Op::Params P;
   if (precision == kFP32Compensated) {
-    P.f = make_frame(origin, sigma, VT<F2>::kScale);
+    P.f = make_frame(origin, sigma, kernel, true);
     fill(P);
-    return run_pairs<Op, F2, TPB32, RT32>(P, n, m, ws, wsb, st);
+    return run_pairs_k<Op, F2, TPB32, RT32>(P, n, m, ws, wsb, st);
   } else if (precision == kFP64) {
-    P.f = make_frame(origin, sigma, VT<double>::kScale);
+    P.f = make_frame(origin, sigma, kernel, false);
     fill(P);
-    return run_pairs<Op, double, kTpb64, kRt64>(P, n, m, ws, wsb, st);
+    return run_pairs_k<Op, double, kTpb64, kRt64>(P, n, m, ws, wsb, st);
   }
   return kInvalidArgument;
 }
 
 template <class Op, int TPB32, int RT32>
 size_t op_ws(int64_t n, int64_t m, int precision) {
-  return precision == kFP32Compensated ? pairs_ws_bytes<Op, F2, TPB32, RT32>(n, m)
-                                       : pairs_ws_bytes<Op, double, kTpb64, kRt64>(n, m);
+  return precision == kFP32Compensated ? pairs_ws_bytes_any<Op, F2, TPB32, RT32>(n, m)
+                                       : pairs_ws_bytes_any<Op, double, kTpb64, kRt64>(n, m);
 }
 
 }  // namespace
@@ -90,57 +91,57 @@ using namespace lddmm;
 
 extern "C" {
 
-int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
+int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma, int kernel,
                   const double* origin, double* out, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(x, m) || bad_ptr(a, m))
     return kInvalidArgument;
-  return dispatch<OpK, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, (cudaStream_t)stream,
+  return dispatch<OpK, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, (cudaStream_t)stream,
                                             [&](OpK::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });
 }
 
 int lddmm_apply_diff_kt(const double* y, int64_t n, const double* x, const double* p, const double* a, int64_t m,
-                        double sigma, int mode, double regweight, const double* origin, double* out, int precision,
-                        void* ws, size_t wsb, lddmm_stream_t stream) {
+                        double sigma, int kernel, int mode, double regweight, const double* origin, double* out,
+                        int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(p, n) || bad_ptr(x, m) ||
       bad_ptr(a, m) || mode < 0 || mode > 2)
     return kInvalidArgument;
   if (mode != 0 && n != m) return kInvalidArgument;
   auto fill = [&](auto& P) { P.y = y; P.x = x; P.p = p; P.a = a; P.out = out; P.w = regweight; };
   cudaStream_t st = (cudaStream_t)stream;
-  if (mode == 0) return dispatch<OpDiffKT<0>, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, st, fill);
-  if (mode == 1) return dispatch<OpDiffKT<1>, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, st, fill);
-  return dispatch<OpDiffKT<2>, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, st, fill);
+  if (mode == 0)
+    return dispatch<OpDiffKT<0>, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, st, fill);
+  if (mode == 1)
+    return dispatch<OpDiffKT<1>, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, st, fill);
+  return dispatch<OpDiffKT<2>, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, st, fill);
 }
 
 int lddmm_apply_ddiff_k11and12(const double* x, const double* nn, const double* a, const double* p, int64_t n,
-                               double sigma, const double* origin, double* out, int precision, void* ws,
+                               double sigma, int kernel, const double* origin, double* out, int precision, void* ws,
                                size_t wsb, lddmm_stream_t stream) {
   if (n < 0 || bad_sigma(sigma) || bad_ptr(x, n) || bad_ptr(nn, n) || bad_ptr(a, n) || bad_ptr(p, n) ||
       bad_ptr(out, n))
     return kInvalidArgument;
-  return dispatch<OpDDiffK, kTpbHeavy, kRtHeavy>(precision, n, n, sigma, origin, ws, wsb, (cudaStream_t)stream,
-                                                 [&](OpDDiffK::Params& P) {
-                                                   P.x = x; P.nn = nn; P.a = a; P.p = p; P.out = out;
-                                                 });
+  auto fill = [&](OpDDiffK::Params& P) { P.x = x; P.nn = nn; P.a = a; P.p = p; P.out = out; };
+  return dispatch<OpDDiffK, kTpbHeavy, kRtHeavy>(precision, n, n, sigma, kernel, origin, ws, wsb,
+                                                 (cudaStream_t)stream, fill);
 }
 
-int lddmm_apply_diff_k1and2(const double* x, const double* a1, const double* a2, int64_t n, double sigma,
+int lddmm_apply_diff_k1and2(const double* x, const double* a1, const double* a2, int64_t n, double sigma, int kernel,
                             const double* origin, double* out, int precision, void* ws, size_t wsb,
                             lddmm_stream_t stream) {
   if (n < 0 || bad_sigma(sigma) || bad_ptr(x, n) || bad_ptr(a1, n) || bad_ptr(a2, n) || bad_ptr(out, n))
     return kInvalidArgument;
-  return dispatch<OpDiffK1and2, kTpbLight, kRtLight>(precision, n, n, sigma, origin, ws, wsb, (cudaStream_t)stream,
-                                                     [&](OpDiffK1and2::Params& P) {
-                                                       P.x = x; P.a1 = a1; P.a2 = a2; P.out = out;
-                                                     });
+  auto fill = [&](OpDiffK1and2::Params& P) { P.x = x; P.a1 = a1; P.a2 = a2; P.out = out; };
+  return dispatch<OpDiffK1and2, kTpbLight, kRtLight>(precision, n, n, sigma, kernel, origin, ws, wsb,
+                                                     (cudaStream_t)stream, fill);
 }
 
 int lddmm_apply_divergence(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
-                           const double* origin, double* out, int precision, void* ws, size_t wsb,
+                           int kernel, const double* origin, double* out, int precision, void* ws, size_t wsb,
                            lddmm_stream_t stream) {
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(x, m) || bad_ptr(a, m))
     return kInvalidArgument;
-  return dispatch<OpDiv, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, (cudaStream_t)stream,
+  return dispatch<OpDiv, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, (cudaStream_t)stream,
                                               [&](OpDiv::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });
 }
 
@@ -150,11 +151,11 @@ int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m,
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(ay, n) || bad_ptr(by, n) || bad_ptr(out, n) ||
       bad_ptr(x, m) || bad_ptr(ax, m) || bad_ptr(bx, m))
     return kInvalidArgument;
-  return dispatch<OpKTensor, kTpbLight, kRtLight>(precision, n, m, sigma, origin, ws, wsb, (cudaStream_t)stream,
-                                                  [&](OpKTensor::Params& P) {
-                                                    P.y = y; P.x = x; P.ay = ay; P.ax = ax; P.by = by; P.bx = bx;
-                                                    P.out = out;
-                                                  });
+  auto fill = [&](OpKTensor::Params& P) {
+    P.y = y; P.x = x; P.ay = ay; P.ax = ax; P.by = by; P.bx = bx; P.out = out;
+  };
+  return dispatch<OpKTensor, kTpbLight, kRtLight>(precision, n, m, sigma, kGauss, origin, ws, wsb,
+                                                  (cudaStream_t)stream, fill);
 }
 
 }  // extern "C"

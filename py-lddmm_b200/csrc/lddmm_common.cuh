@@ -151,13 +151,74 @@ __device__ __forceinline__ double partial_value(double p) { return p; }
 
 __device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
 
-// Geometry shared by every op: centred, pre-scaled coordinates.
+// Kernel families (the `kernel` argument of the C ABI): 0 = Gaussian, 16 + q = Laplacian (Matern) of order q <= 4,
+// K(r) = P_q(r / sigma) exp(-r / sigma) (base/kernelFunctions_util.py:20-52 lapPol / lapPolDiff / lapPolDiff2).
+enum KernelFamily : int { kGauss = 0, kLaplacian0 = 16, kLaplacianMax = 20 };
+
+// Geometry shared by every op: centred, pre-scaled coordinates, and the radial profile of the kernel.
 struct Frame {
   double o0, o1, o2;  // origin subtracted before scaling
-  double s;           // coordinate scale (kScale / sigma)
+  double s;           // coordinate scale (Gaussian: kScale / sigma; Laplacian: 1/sigma, times log2(e) in FP32)
   double kappa;       // 1 / (s sigma^2): turns a scaled difference into (y - x) / sigma^2
   double inv_s2;      // 1 / sigma^2
+  int family;         // KernelFamily
+  // Laplacian profile in the scaled radius u' = |d|: K0 = P0(u') E, K1 = P1(u') E, K2 = P2(u') E with
+  // E = exp(-u') (FP64) or 2^-u' (FP32, coefficients rescaled). grad_y K = -K1 kappa d, Hessian = kappa^2 K2 d d^T
+  // - K1/sigma^2 I. Row r holds the coefficients of P_r in increasing degree (zeros past the order).
+  float lc[3][5];
+  double dc[3][5];
 };
+
+// Radial factors of one pair: K0 (value), K1 (first-derivative factor), K2 (second-derivative factor). For the
+// Gaussian all three are exp(-|d|^2); unused ones are removed by the compiler.
+template <typename V>
+struct KV {
+  V k0, k1, k2;
+};
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct Gauss {
+  template <typename V>
+  static __device__ __forceinline__ KV<V> eval(const Frame&, V r2) {
+    const V e = VT<V>::expneg(r2);
+    return {e, e, e};
+  }
+};
+
+struct Laplacian {
+  template <typename V>
+  static __device__ __forceinline__ KV<V> eval(const Frame& f, V r2);
+};
+
+__device__ __forceinline__ float horner5(const float* c, float u) {
+  return fmaf(fmaf(fmaf(fmaf(c[4], u, c[3]), u, c[2]), u, c[1]), u, c[0]);
+}
+__device__ __forceinline__ double horner5(const double* c, double u) {
+  return ::fma(::fma(::fma(::fma(c[4], u, c[3]), u, c[2]), u, c[1]), u, c[0]);
+}
+
+template <>
+__device__ __forceinline__ KV<F2> Laplacian::eval<F2>(const Frame& f, F2 r2) {
+  float a, b;
+  split(r2, a, b);
+  const float ua = sqrt_approx(a), ub = sqrt_approx(b);
+  const float ea = ex2neg(ua), eb = ex2neg(ub);
+  KV<F2> k;
+  k.k0 = f2(ea * horner5(f.lc[0], ua), eb * horner5(f.lc[0], ub));
+  k.k1 = f2(ea * horner5(f.lc[1], ua), eb * horner5(f.lc[1], ub));
+  k.k2 = f2(ea * horner5(f.lc[2], ua), eb * horner5(f.lc[2], ub));
+  return k;
+}
+template <>
+__device__ __forceinline__ KV<double> Laplacian::eval<double>(const Frame& f, double r2) {
+  const double u = sqrt(r2), e = exp(-u);
+  return {e * horner5(f.dc[0], u), e * horner5(f.dc[1], u), e * horner5(f.dc[2], u)};
+}
 
 // Shared-memory unit: two source fields (each a duplicated FP32 pair or one FP64 value), 16 bytes.
 template <typename V>
@@ -230,10 +291,10 @@ inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int 
 //   Op::template Tgt<V>                                  per-lane-group register state
 //   Op::template load_target<V>(P, i0, i1, tgt)          (i0, i1 < n; i1 ignored for V = double)
 //   Op::source_fields(P, l, double* f)                   the NS source fields of source l (l < m), FP64
-//   Op::template pair<V>(tgt, const V* s, V* acc)
+//   Op::template pair<V, Fam>(const Frame&, tgt, const V* s, V* acc)   (Fam: Gauss or Laplacian)
 // Output: ws[(slot * NA + c) * n + i] = compensated partial of accumulator c of target i for one segment.
 // ---------------------------------------------------------------------------------------------------------
-template <class Op, typename V, int TPB, int RT>
+template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
     pairs_kernel(const typename Op::Params P, int n, int m, int TT, long long W, int C,
                  typename VT<V>::Partial* __restrict__ ws) {
@@ -296,7 +357,7 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
           s[2 * q + 1] = w.b;
         }
 #pragma unroll
-        for (int g = 0; g < G; ++g) Op::template pair<V>(tgt[g], s, acc[g]);
+        for (int g = 0; g < G; ++g) Op::template pair<V, Fam>(P.f, tgt[g], s, acc[g]);
       }
 #pragma unroll
       for (int g = 0; g < G; ++g)
@@ -344,47 +405,99 @@ __global__ void ordered_sum_kernel(const double* __restrict__ v, int count, doub
 
 int resident_ctas(const void* kernel, int threads);
 
-template <class Op, typename V, int TPB, int RT>
+template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline int ctas_per_sm() {
   static int cached = 0;
   if (cached == 0) {
-    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel<Op, V, TPB, RT>), TPB);
+    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel<Op, V, TPB, RT, Fam>), TPB);
     cached = c > 0 ? c : 4;
   }
   return cached;
 }
 
-template <class Op, typename V, int TPB, int RT>
+template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* ws, size_t ws_bytes,
                      cudaStream_t stream) {
   if (n <= 0) return kOk;
   if (n > INT32_MAX / 4 || m > INT32_MAX / 4) return kInvalidArgument;
-  SKPlan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT>());
+  SKPlan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial),
+                                   ctas_per_sm<Op, V, TPB, RT, Fam>());
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (plan.ws_bytes > 0 && ws == nullptr) return kInvalidArgument;
   auto* part = reinterpret_cast<typename VT<V>::Partial*>(ws);
   if (plan.W > 0)
-    pairs_kernel<Op, V, TPB, RT><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C, part);
+    pairs_kernel<Op, V, TPB, RT, Fam><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C,
+                                                                   part);
   const int fb = 256;
   finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, TPB * RT, plan.TT, plan.W, plan.C,
                                                                       part);
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
-template <class Op, typename V, int TPB, int RT>
+template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline size_t pairs_ws_bytes(int64_t n, int64_t m) {
-  return make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT>()).ws_bytes;
+  return make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT, Fam>())
+      .ws_bytes;
 }
 
-inline Frame make_frame(const double* origin, double sigma, double kscale) {
-  Frame f;
+// Workspace of an op for every kernel family (the larger of the Gaussian and Laplacian plans).
+template <class Op, typename V, int TPB, int RT>
+inline size_t pairs_ws_bytes_any(int64_t n, int64_t m) {
+  const size_t a = pairs_ws_bytes<Op, V, TPB, RT, Gauss>(n, m), b = pairs_ws_bytes<Op, V, TPB, RT, Laplacian>(n, m);
+  return a > b ? a : b;
+}
+
+inline bool bad_kernel(int kernel) { return !(kernel == kGauss || (kernel >= kLaplacian0 && kernel <= kLaplacianMax)); }
+
+// Frame of one kernel width. `fp32` selects the FP32 scaling (exp2-based) or the FP64 one (exp-based).
+inline Frame make_frame(const double* origin, double sigma, int kernel, bool fp32) {
+  Frame f = {};
+  f.family = kernel;
   f.o0 = origin ? origin[0] : 0.0;
   f.o1 = origin ? origin[1] : 0.0;
   f.o2 = origin ? origin[2] : 0.0;
-  f.s = kscale / sigma;
+  constexpr double kLog2e = 1.44269504088896340736;
+  if (kernel == kGauss) {
+    f.s = (fp32 ? VT<F2>::kScale : VT<double>::kScale) / sigma;
+  } else {
+    // P0 = lapPol of the order (Matern polynomial); P1 = (P0 - P0') / u and P2 = (P1 - P1') / u when the division
+    // is exact (the constant terms cancel), else zero -- the reference's derivative tables for orders 0 and 1.
+    static const double kP0[5][5] = {{1, 0, 0, 0, 0},
+                                     {1, 1, 0, 0, 0},
+                                     {1, 1, 1.0 / 3, 0, 0},
+                                     {1, 1, 0.4, 1.0 / 15, 0},
+                                     {1, 1, 3.0 / 7, 2.0 / 21, 1.0 / 105}};
+    const int q = kernel - kLaplacian0;
+    double c[3][5] = {};
+    for (int k = 0; k < 5; ++k) c[0][k] = kP0[q][k];
+    for (int r = 1; r < 3; ++r) {
+      double d[5] = {};  // c[r-1] - derivative of c[r-1]
+      for (int k = 0; k < 5; ++k) d[k] = c[r - 1][k] - (k + 1 < 5 ? (k + 1) * c[r - 1][k + 1] : 0.0);
+      if (d[0] > -1e-12 && d[0] < 1e-12)  // exact in rationals; rounding leaves ~1e-17
+        for (int k = 0; k < 4; ++k) c[r][k] = d[k + 1];
+    }
+    const double unit = fp32 ? kLog2e : 1.0;  // FP32 works in u' = log2(e) u so that E = 2^-u'
+    f.s = unit / sigma;
+    double pw = 1.0;
+    for (int k = 0; k < 5; ++k) {
+      for (int r = 0; r < 3; ++r) {
+        f.dc[r][k] = c[r][k] * pw;
+        f.lc[r][k] = (float)(c[r][k] * pw);
+      }
+      pw /= unit;
+    }
+  }
   f.kappa = 1.0 / (f.s * sigma * sigma);
   f.inv_s2 = 1.0 / (sigma * sigma);
   return f;
+}
+
+// Launch an op with the pair kernel of its frame's family (P.f.family).
+template <class Op, typename V, int TPB, int RT>
+inline int run_pairs_k(const typename Op::Params& P, int64_t n, int64_t m, void* ws, size_t ws_bytes,
+                       cudaStream_t stream) {
+  if (P.f.family == kGauss) return run_pairs<Op, V, TPB, RT, Gauss>(P, n, m, ws, ws_bytes, stream);
+  return run_pairs<Op, V, TPB, RT, Laplacian>(P, n, m, ws, ws_bytes, stream);
 }
 
 inline bool bad_sigma(double sigma) { return !(sigma > 0.0) || !(sigma < 1e300); }

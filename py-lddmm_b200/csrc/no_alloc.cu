@@ -80,9 +80,9 @@ extern "C" int lddmm_apply_k_static(const double* y, int64_t n, const double* x,
   P.out = out;
   cudaStream_t st = (cudaStream_t)stream;
   if (precision == kFP32Compensated) {
-    P.f = make_frame(origin, sigma, VT<F2>::kScale);
+    P.f = make_frame(origin, sigma, kGauss, true);
     return run_pairs<OpK, F2, kTpbLight, kRtLight>(P, n, m, scratch, kStaticScratchBytes, st);
   }
-  P.f = make_frame(origin, sigma, VT<double>::kScale);
+  P.f = make_frame(origin, sigma, kGauss, false);
   return run_pairs<OpK, double, kTpb64, kRt64>(P, n, m, scratch, kStaticScratchBytes, st);
 }

@@ -36,14 +36,14 @@ struct OpSOFwd {
     src_point(P.x, l, P.f, f);
     f[3] = P.a[3 * l]; f[4] = P.a[3 * l + 1]; f[5] = P.a[3 * l + 2];
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
-    acc[0] = fma(e, s[3], acc[0]);
-    acc[1] = fma(e, s[4], acc[1]);
-    acc[2] = fma(e, s[5], acc[2]);
-    const V ec = e * dot3(t.a0, t.a1, t.a2, s[3], s[4], s[5]);
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
+    acc[0] = fma(k.k0, s[3], acc[0]);
+    acc[1] = fma(k.k0, s[4], acc[1]);
+    acc[2] = fma(k.k0, s[5], acc[2]);
+    const V ec = k.k1 * dot3(t.a0, t.a1, t.a2, s[3], s[4], s[5]);
     acc[3] = fma(ec, d0, acc[3]);
     acc[4] = fma(ec, d1, acc[4]);
     acc[5] = fma(ec, d2, acc[5]);
@@ -109,26 +109,26 @@ struct OpSOBwd {
       f[9 + c] = -k * P.px[3 * l + c];
     }
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
     const V dq = dot3(d0, d1, d2, t.q0 - s[6], t.q1 - s[7], t.q2 - s[8]);
     const V c1 = fma(t.a2, s[11], fma(t.a1, s[10], fma(t.a0, s[9], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
     const V c2 = dot3(t.b0, t.b1, t.b2, s[3], s[4], s[5]);
-    const V eg = e * fma(c2, dq, c1);
+    const V ec2 = k.k1 * c2;
+    const V eg = fma(k.k2 * c2, dq, k.k1 * c1);  // Gaussian: e (c1 + c2 dq), k2 * c2 == ec2
     acc[0] = fma(eg, d0, acc[0]);
     acc[1] = fma(eg, d1, acc[1]);
     acc[2] = fma(eg, d2, acc[2]);
-    const V ec2 = e * c2;
     acc[3] = acc[3] + ec2;
     acc[4] = fma(ec2, s[6], acc[4]);
     acc[5] = fma(ec2, s[7], acc[5]);
     acc[6] = fma(ec2, s[8], acc[6]);
-    acc[7] = fma(e, s[9], acc[7]);
-    acc[8] = fma(e, s[10], acc[8]);
-    acc[9] = fma(e, s[11], acc[9]);
-    const V edq = e * dq;
+    acc[7] = fma(k.k0, s[9], acc[7]);
+    acc[8] = fma(k.k0, s[10], acc[8]);
+    acc[9] = fma(k.k0, s[11], acc[9]);
+    const V edq = k.k1 * dq;
     acc[10] = fma(edq, s[3], acc[10]);
     acc[11] = fma(edq, s[4], acc[11]);
     acc[12] = fma(edq, s[5], acc[12]);
@@ -181,18 +181,18 @@ struct OpFOBwd {
       f[6 + c] = P.p[3 * l + c] - 2.0 * P.w * P.a[3 * l + c];
     }
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
     const V c = fma(t.a2, s[8], fma(t.a1, s[7], fma(t.a0, s[6], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
-    const V ec = e * c;
+    const V ec = k.k1 * c;
     acc[0] = fma(ec, d0, acc[0]);
     acc[1] = fma(ec, d1, acc[1]);
     acc[2] = fma(ec, d2, acc[2]);
-    acc[3] = fma(e, s[6], acc[3]);
-    acc[4] = fma(e, s[7], acc[4]);
-    acc[5] = fma(e, s[8], acc[5]);
+    acc[3] = fma(k.k0, s[6], acc[3]);
+    acc[4] = fma(k.k0, s[7], acc[4]);
+    acc[5] = fma(k.k0, s[8], acc[5]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = P.dt * P.f.kappa;
@@ -208,15 +208,15 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
   size_t b = 0;
   auto upd = [&](size_t v) { b = v > b ? v : b; };
   if (precision == kFP32Compensated) {
-    upd(pairs_ws_bytes<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
-    upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtHeavy>(n, n));
-    upd(pairs_ws_bytes<OpFOBwd, F2, kTpbLight, kRtLight>(n, n));
-    upd(pairs_ws_bytes<OpK, F2, kTpbLight, kRtLight>(n, n));
+    upd(pairs_ws_bytes_any<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
+    upd(pairs_ws_bytes_any<OpSOBwd, F2, kTpbHeavy, kRtHeavy>(n, n));
+    upd(pairs_ws_bytes_any<OpFOBwd, F2, kTpbLight, kRtLight>(n, n));
+    upd(pairs_ws_bytes_any<OpK, F2, kTpbLight, kRtLight>(n, n));
   } else {
-    upd(pairs_ws_bytes<OpSOFwd, double, kTpb64, kRt64>(n, n));
-    upd(pairs_ws_bytes<OpSOBwd, double, kTpb64, kRt64>(n, n));
-    upd(pairs_ws_bytes<OpFOBwd, double, kTpb64, kRt64>(n, n));
-    upd(pairs_ws_bytes<OpK, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes_any<OpSOFwd, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes_any<OpSOBwd, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes_any<OpFOBwd, double, kTpb64, kRt64>(n, n));
+    upd(pairs_ws_bytes_any<OpK, double, kTpb64, kRt64>(n, n));
   }
   // per-point dot products for the FP64 energy reductions live after the pair partials
   return ((b + 255) & ~(size_t)255) + (size_t)(n > 0 ? n : 0) * sizeof(double);
@@ -234,8 +234,8 @@ template <> struct Shape<double> {
 };
 
 template <typename V>
-inline Frame frame(const double* origin, double sigma) {
-  return make_frame(origin, sigma, VT<V>::kScale);
+inline Frame frame(const double* origin, double sigma, int kernel) {
+  return make_frame(origin, sigma, kernel, VT<V>::kLanes == 2);
 }
 
 inline double* dots_region(void* ws, size_t pair_bytes) {
@@ -252,13 +252,13 @@ int k_energy_and_update(const double* x, const double* a, int64_t n, const Frame
   OpK::Params P;
   P.y = x; P.x = x; P.a = a; P.out = out; P.f = f;
   P.base = base; P.base_sign = base_sign; P.scale = scale;
-  const size_t pb = pairs_ws_bytes<OpK, V, TPB, RT>(n, n);
+  const size_t pb = pairs_ws_bytes_any<OpK, V, TPB, RT>(n, n);
   if (energy) {
     if (((pb + 255) & ~(size_t)255) + (size_t)n * sizeof(double) > wsb) return kWorkspaceTooSmall;
     P.dotw = dotw;
     P.dots = dots_region(ws, pb);
   }
-  int rc = run_pairs<OpK, V, TPB, RT>(P, n, n, ws, wsb, st);
+  int rc = run_pairs_k<OpK, V, TPB, RT>(P, n, n, ws, wsb, st);
   if (rc != kOk) return rc;
   if (energy) {
     ordered_sum_kernel<<<1, 1024, 0, st>>>(P.dots, (int)n, escale, energy, accumulate);
@@ -271,7 +271,7 @@ template <typename V>
 int so_step(const double* x, const double* a, int64_t n, const Frame& f, double dt, double* x1, double* a1, void* ws,
             size_t wsb, cudaStream_t st, int64_t row0 = 0, int64_t nrows = -1) {
   OpSOFwd::Params P{x, a, x1, a1, f, dt, (int)row0};
-  return run_pairs<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
+  return run_pairs_k<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
 }
 
 template <typename V>
@@ -279,7 +279,7 @@ int so_adjoint_step(const double* x, const double* a, const double* px, const do
                     double dt, double* px_prev, double* pa_prev, void* ws, size_t wsb, cudaStream_t st,
                     int64_t row0 = 0, int64_t nrows = -1) {
   OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt, (int)row0};
-  return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
+  return run_pairs_k<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
 }
 
 template <typename V>
@@ -343,7 +343,7 @@ int fo_gradient(const double* xt, const double* at, int64_t n, int64_t T, const 
   for (int64_t t = T - 1; t >= 0; --t) {
     OpFOBwd::Params P{xt + t * stride, at + t * stride, pxt + (t + 1) * stride, pxt + t * stride, dat + t * stride,
                       f, dt, regweight, euclidean};
-    int rc = run_pairs<OpFOBwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
+    int rc = run_pairs_k<OpFOBwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
     if (rc != kOk) return rc;
   }
   return kOk;
@@ -356,109 +356,113 @@ bool bad(const void* p, int64_t n) { return n > 0 && p == nullptr; }
 
 using namespace lddmm;
 
-#define LDDMM_DISPATCH(precision, call_f2, call_f64) \
-  ((precision) == kFP32Compensated ? (call_f2) : ((precision) == kFP64 ? (call_f64) : (int)kInvalidArgument))
+namespace {
+
+// Runs fn(V{}, frame) with V = F2 (FP32 path) or double (FP64 path).
+template <class Fn>
+int by_precision(int precision, const double* origin, double sigma, int kernel, Fn&& fn) {
+  if (precision == kFP32Compensated) return fn(F2{}, frame<F2>(origin, sigma, kernel));
+  if (precision == kFP64) return fn(0.0, frame<double>(origin, sigma, kernel));
+  return kInvalidArgument;
+}
+
+bool bad_width(double sigma, int kernel) { return bad_sigma(sigma) || bad_kernel(kernel); }
+
+}  // namespace
 
 extern "C" {
 
-int lddmm_second_order_step(const double* x, const double* a, int64_t n, double sigma, double dt,
-                            const double* origin, double* x_next, double* a_next, int precision, void* ws,
-                            size_t wsb, lddmm_stream_t stream) {
-  if (n < 0 || bad_sigma(sigma) || bad(x, n) || bad(a, n) || bad(x_next, n) || bad(a_next, n)) return kInvalidArgument;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(precision, so_step<F2>(x, a, n, frame<F2>(origin, sigma), dt, x_next, a_next, ws, wsb, st),
-                        so_step<double>(x, a, n, frame<double>(origin, sigma), dt, x_next, a_next, ws, wsb, st));
+int lddmm_second_order_step(const double* x, const double* a, int64_t n, double sigma, int kernel, double dt,
+                            const double* origin, double* x_next, double* a_next, int precision, void* ws, size_t wsb,
+                            lddmm_stream_t stream) {
+  if (n < 0 || bad_width(sigma, kernel) || bad(x, n) || bad(a, n) || bad(x_next, n) || bad(a_next, n))
+    return kInvalidArgument;
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return so_step<decltype(v)>(x, a, n, f, dt, x_next, a_next, ws, wsb, (cudaStream_t)stream);
+  });
 }
 
-int lddmm_second_order_step_rows(const double* x, const double* a, int64_t n, int64_t row0, int64_t nrows,
-                                 double sigma, double dt, const double* origin, double* x_next_rows,
-                                 double* a_next_rows, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
-  if (n < 0 || row0 < 0 || nrows < 0 || row0 + nrows > n || bad_sigma(sigma) || bad(x, n) || bad(a, n) ||
+int lddmm_second_order_step_rows(const double* x, const double* a, int64_t n, int64_t row0, int64_t nrows, double sigma,
+                                 int kernel, double dt, const double* origin, double* x_next_rows, double* a_next_rows,
+                                 int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || row0 < 0 || nrows < 0 || row0 + nrows > n || bad_width(sigma, kernel) || bad(x, n) || bad(a, n) ||
       bad(x_next_rows, nrows) || bad(a_next_rows, nrows))
     return kInvalidArgument;
   if (nrows == 0) return kOk;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(precision,
-                        so_step<F2>(x, a, n, frame<F2>(origin, sigma), dt, x_next_rows, a_next_rows, ws, wsb, st,
-                                    row0, nrows),
-                        so_step<double>(x, a, n, frame<double>(origin, sigma), dt, x_next_rows, a_next_rows, ws, wsb,
-                                        st, row0, nrows));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return so_step<decltype(v)>(x, a, n, f, dt, x_next_rows, a_next_rows, ws, wsb, (cudaStream_t)stream, row0, nrows);
+  });
 }
 
-int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int64_t T, double sigma, double dt,
-                             const double* origin, double* xt, double* at, int precision, void* ws, size_t wsb,
-                             lddmm_stream_t stream) {
-  if (n < 0 || T < 0 || bad_sigma(sigma) || bad(x0, n) || bad(a0, n) || bad(xt, n) || bad(at, n)) return kInvalidArgument;
+int lddmm_second_order_shoot(const double* x0, const double* a0, int64_t n, int64_t T, double sigma, int kernel,
+                             double dt, const double* origin, double* xt, double* at, int precision, void* ws,
+                             size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || T < 0 || bad_width(sigma, kernel) || bad(x0, n) || bad(a0, n) || bad(xt, n) || bad(at, n))
+    return kInvalidArgument;
   if (n == 0) return kOk;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(precision, so_shoot<F2>(x0, a0, n, T, frame<F2>(origin, sigma), dt, xt, at, ws, wsb, st),
-                        so_shoot<double>(x0, a0, n, T, frame<double>(origin, sigma), dt, xt, at, ws, wsb, st));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return so_shoot<decltype(v)>(x0, a0, n, T, f, dt, xt, at, ws, wsb, (cudaStream_t)stream);
+  });
 }
 
 int lddmm_second_order_adjoint_step(const double* x, const double* a, const double* px, const double* pa, int64_t n,
-                                    double sigma, double dt, const double* origin, double* px_prev, double* pa_prev,
-                                    int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
-  if (n < 0 || bad_sigma(sigma) || bad(x, n) || bad(a, n) || bad(px, n) || bad(pa, n) || bad(px_prev, n) ||
+                                    double sigma, int kernel, double dt, const double* origin, double* px_prev,
+                                    double* pa_prev, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || bad_width(sigma, kernel) || bad(x, n) || bad(a, n) || bad(px, n) || bad(pa, n) || bad(px_prev, n) ||
       bad(pa_prev, n))
     return kInvalidArgument;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(
-      precision, so_adjoint_step<F2>(x, a, px, pa, n, frame<F2>(origin, sigma), dt, px_prev, pa_prev, ws, wsb, st),
-      so_adjoint_step<double>(x, a, px, pa, n, frame<double>(origin, sigma), dt, px_prev, pa_prev, ws, wsb, st));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return so_adjoint_step<decltype(v)>(x, a, px, pa, n, f, dt, px_prev, pa_prev, ws, wsb, (cudaStream_t)stream);
+  });
 }
 
 int lddmm_second_order_adjoint_step_rows(const double* x, const double* a, const double* px, const double* pa,
-                                         int64_t n, int64_t row0, int64_t nrows, double sigma, double dt,
+                                         int64_t n, int64_t row0, int64_t nrows, double sigma, int kernel, double dt,
                                          const double* origin, double* px_prev_rows, double* pa_prev_rows,
                                          int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
-  if (n < 0 || row0 < 0 || nrows < 0 || row0 + nrows > n || bad_sigma(sigma) || bad(x, n) || bad(a, n) ||
+  if (n < 0 || row0 < 0 || nrows < 0 || row0 + nrows > n || bad_width(sigma, kernel) || bad(x, n) || bad(a, n) ||
       bad(px, n) || bad(pa, n) || bad(px_prev_rows, nrows) || bad(pa_prev_rows, nrows))
     return kInvalidArgument;
   if (nrows == 0) return kOk;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(precision,
-                        so_adjoint_step<F2>(x, a, px, pa, n, frame<F2>(origin, sigma), dt, px_prev_rows,
-                                            pa_prev_rows, ws, wsb, st, row0, nrows),
-                        so_adjoint_step<double>(x, a, px, pa, n, frame<double>(origin, sigma), dt, px_prev_rows,
-                                                pa_prev_rows, ws, wsb, st, row0, nrows));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return so_adjoint_step<decltype(v)>(x, a, px, pa, n, f, dt, px_prev_rows, pa_prev_rows, ws, wsb,
+                                        (cudaStream_t)stream, row0, nrows);
+  });
 }
 
-int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, double dt,
-                                const double* px1, const double* pa1, const double* origin, double* pxt, double* pat,
-                                double* da0, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
-  if (n < 0 || T < 0 || bad_sigma(sigma) || bad(xt, n) || bad(at, n) || bad(px1, n) || bad(pa1, n) || bad(pxt, n) ||
-      bad(pat, n))
+int lddmm_second_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, int kernel,
+                                double dt, const double* px1, const double* pa1, const double* origin, double* pxt,
+                                double* pat, double* da0, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || T < 0 || bad_width(sigma, kernel) || bad(xt, n) || bad(at, n) || bad(px1, n) || bad(pa1, n) ||
+      bad(pxt, n) || bad(pat, n))
     return kInvalidArgument;
   if (n == 0) return kOk;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(
-      precision, so_gradient<F2>(xt, at, n, T, frame<F2>(origin, sigma), dt, px1, pa1, pxt, pat, da0, ws, wsb, st),
-      so_gradient<double>(xt, at, n, T, frame<double>(origin, sigma), dt, px1, pa1, pxt, pat, da0, ws, wsb, st));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return so_gradient<decltype(v)>(xt, at, n, T, f, dt, px1, pa1, pxt, pat, da0, ws, wsb, (cudaStream_t)stream);
+  });
 }
 
-int lddmm_first_order_shoot(const double* x0, const double* at, int64_t n, int64_t T, double sigma, double regweight,
-                            const double* origin, double* xt, double* energy, int precision, void* ws, size_t wsb,
-                            lddmm_stream_t stream) {
-  if (n < 0 || T < 0 || bad_sigma(sigma) || bad(x0, n) || bad(at, n) || bad(xt, n)) return kInvalidArgument;
+int lddmm_first_order_shoot(const double* x0, const double* at, int64_t n, int64_t T, double sigma, int kernel,
+                            double regweight, const double* origin, double* xt, double* energy, int precision, void* ws,
+                            size_t wsb, lddmm_stream_t stream) {
+  if (n < 0 || T < 0 || bad_width(sigma, kernel) || bad(x0, n) || bad(at, n) || bad(xt, n)) return kInvalidArgument;
   if (n == 0) return kOk;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(
-      precision, fo_shoot<F2>(x0, at, n, T, frame<F2>(origin, sigma), regweight, xt, energy, ws, wsb, st),
-      fo_shoot<double>(x0, at, n, T, frame<double>(origin, sigma), regweight, xt, energy, ws, wsb, st));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return fo_shoot<decltype(v)>(x0, at, n, T, f, regweight, xt, energy, ws, wsb, (cudaStream_t)stream);
+  });
 }
 
-int lddmm_first_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma,
+int lddmm_first_order_gradient(const double* xt, const double* at, int64_t n, int64_t T, double sigma, int kernel,
                                double regweight, const double* px1, int euclidean, const double* origin, double* pxt,
                                double* dat, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
-  if (n < 0 || T < 0 || bad_sigma(sigma) || bad(xt, n) || bad(at, n) || bad(px1, n) || bad(pxt, n) || bad(dat, n))
+  if (n < 0 || T < 0 || bad_width(sigma, kernel) || bad(xt, n) || bad(at, n) || bad(px1, n) || bad(pxt, n) ||
+      bad(dat, n))
     return kInvalidArgument;
   if (n == 0) return kOk;
-  cudaStream_t st = (cudaStream_t)stream;
-  return LDDMM_DISPATCH(
-      precision,
-      fo_gradient<F2>(xt, at, n, T, frame<F2>(origin, sigma), regweight, px1, euclidean, pxt, dat, ws, wsb, st),
-      fo_gradient<double>(xt, at, n, T, frame<double>(origin, sigma), regweight, px1, euclidean, pxt, dat, ws, wsb,
-                          st));
+  return by_precision(precision, origin, sigma, kernel, [&](auto v, const Frame& f) {
+    return fo_gradient<decltype(v)>(xt, at, n, T, f, regweight, px1, euclidean, pxt, dat, ws, wsb,
+                                    (cudaStream_t)stream);
+  });
 }
 
 }  // extern "C"

@@ -112,10 +112,10 @@ struct OpSurfEnergy {
   static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
     face_source_fields<KIND>(P.S, P.f, l, f);
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame&, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));  // Gaussian data kernel
     if (KIND == LDDMM_DATA_VARIFOLD) {
       const V g = dot3(t.n0, t.n1, t.n2, s[4], s[5], s[6]);
       const V ea = e * s[3];
@@ -161,10 +161,10 @@ struct OpSurfGrad {
   static __device__ __forceinline__ void source_fields(const Params& P, int l, double* f) {
     face_source_fields<KIND>(P.S, P.f, l, f);
   }
-  template <typename V>
-  static __device__ __forceinline__ void pair(const Tgt<V>& t, const V* s, V* acc) {
+  template <typename V, class Fam>
+  static __device__ __forceinline__ void pair(const Frame&, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const V e = VT<V>::expneg(sqdist(d0, d1, d2));
+    const V e = VT<V>::expneg(sqdist(d0, d1, d2));  // Gaussian data kernel
     if (KIND == LDDMM_DATA_VARIFOLD) {
       const V g = dot3(t.n0, t.n1, t.n2, s[4], s[5], s[6]);
       const V ea = e * s[3];
@@ -323,9 +323,9 @@ int surf_energy_dispatch(int precision, const FaceRec* def, int nf, const FaceRe
                          double sigma, int with_norm0, double* energy, double* dots, void* pairs, size_t pb,
                          cudaStream_t st) {
   if (precision == kFP32Compensated)
-    return surf_energy<F2, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<F2>::kScale),
+    return surf_energy<F2, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, kGauss, true),
                                                       with_norm0, energy, dots, pairs, pb, st);
-  return surf_energy<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<double>::kScale),
+  return surf_energy<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, kGauss, false),
                                                   with_norm0, energy, dots, pairs, pb, st);
 }
 
@@ -333,9 +333,9 @@ template <int KIND>
 int surf_grad_dispatch(int precision, const FaceRec* def, int nf, const FaceRec* tgt, int nf1, const double* origin,
                        double sigma, FaceGrad* grads, void* pairs, size_t pb, cudaStream_t st) {
   if (precision == kFP32Compensated)
-    return surf_grad<F2, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<F2>::kScale),
+    return surf_grad<F2, kTpbLight, kRtLight, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, kGauss, true),
                                                     grads, pairs, pb, st);
-  return surf_grad<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, VT<double>::kScale),
+  return surf_grad<double, kTpb64, kRt64, KIND>(def, nf, tgt, nf1, make_frame(origin, sigma, kGauss, false),
                                                 grads, pairs, pb, st);
 }
 

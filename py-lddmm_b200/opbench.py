@@ -1,10 +1,12 @@
 """Per-operator timing of the hot kernels on synthetic icosphere inputs.
 
     python py-lddmm_b200/opbench.py [--level 6] [--ops all] [--precision fp32|fp64] [--reps 10] [--warmup 3]
+                                    [--kernel gauss|laplacian:<order>]
 
 For every operator: device time per call (CUDA events on the launching stream, after warm-up), pair evaluations
 per second, FP32 lane-ops per second from the per-pair operation counts of the kernel, and the fraction of the
-FP32 pipe peak (SMs x 128 lanes x max SM clock). One JSON line per operator. Used for the ncu captures in
+FP32 pipe peak (SMs x 128 lanes x max SM clock); the operation counts are those of the Gaussian kernel, so with
+--kernel laplacian only times and pairs/s are reported. One JSON line per operator. Used for the ncu captures in
 profiles/ (run it with --reps 1 --warmup 0 under ncu to capture one launch per operator).
 """
 import argparse
@@ -38,7 +40,9 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--sigma', type=float, default=0.5)
     ap.add_argument('--sigma-dist', type=float, default=0.2)
+    ap.add_argument('--kernel', default='gauss', help="deformation kernel: 'gauss' or 'laplacian:<order>'")
     args = ap.parse_args()
+    kern = nat.KERNEL_GAUSS if args.kernel == 'gauss' else nat.KERNEL_LAPLACIAN0 + int(args.kernel.split(':')[1])
     prec = nat.FP32C if args.precision == 'fp32' else nat.FP64
     lib = nat.lib()
     x, F = icosphere(args.level)
@@ -66,19 +70,17 @@ def main():
             raise RuntimeError(lib.lddmm_status_string(rc).decode())
 
     calls = {
-        'applyK': (lambda: ok(lib.lddmm_apply_k(p(X), n, p(X), p(A), n, s, o, p(o1), prec, ws, wsb, st))),
-        'applyDiffKT_lddmm': (lambda: ok(lib.lddmm_apply_diff_kt(p(X), n, p(X), p(P), p(A), n, s, 2, 1.0, o, p(o1),
-                                                                   prec, ws, wsb, st))),
-        'applyDDiffK11and12': (lambda: ok(lib.lddmm_apply_ddiff_k11and12(p(X), p(A), p(A), p(Q), n, s, o, p(o1), prec,
-                                                                         ws, wsb, st))),
-        'applyDiffK1and2': (lambda: ok(lib.lddmm_apply_diff_k1and2(p(X), p(Q), p(A), n, s, o, p(o1), prec, ws, wsb,
-                                                                   st))),
-        'so_step': (lambda: ok(lib.lddmm_second_order_step(p(X), p(A), n, s, 0.05, o, p(o1), p(o2), prec, ws, wsb,
-                                                           st))),
-        'so_adjoint_step': (lambda: ok(lib.lddmm_second_order_adjoint_step(p(X), p(A), p(P), p(Q), n, s, 0.05, o,
-                                                                           p(o1), p(o2), prec, ws, wsb, st))),
-        'fo_adjoint_step': (lambda: ok(lib.lddmm_first_order_gradient(p(X), p(A), n, 0, s, 1.0, p(P), 1, o, p(o1),
-                                                                      p(dat), prec, ws, wsb, st))),
+        'applyK': (lambda: ok(lib.lddmm_apply_k(p(X), n, p(X), p(A), n, s, kern, o, p(o1), prec, ws, wsb, st))),
+        'applyDiffKT_lddmm': (lambda: ok(lib.lddmm_apply_diff_kt(p(X), n, p(X), p(P), p(A), n, s, kern, 2, 1.0, o,
+                                                                   p(o1), prec, ws, wsb, st))),
+        'applyDDiffK11and12': (lambda: ok(lib.lddmm_apply_ddiff_k11and12(p(X), p(A), p(A), p(Q), n, s, kern, o, p(o1),
+                                                                         prec, ws, wsb, st))),
+        'applyDiffK1and2': (lambda: ok(lib.lddmm_apply_diff_k1and2(p(X), p(Q), p(A), n, s, kern, o, p(o1), prec, ws,
+                                                                   wsb, st))),
+        'so_step': (lambda: ok(lib.lddmm_second_order_step(p(X), p(A), n, s, kern, 0.05, o, p(o1), p(o2), prec, ws,
+                                                           wsb, st))),
+        'so_adjoint_step': (lambda: ok(lib.lddmm_second_order_adjoint_step(p(X), p(A), p(P), p(Q), n, s, kern, 0.05,
+                                                                           o, p(o1), p(o2), prec, ws, wsb, st))),
         'varifold_energy': (lambda: ok(lib.lddmm_surface_energy(0, p(X), n, p(FF), nf, None, p(X1), n, p(FF), nf, None,
                                                                 sd, o, 0, p(E), prec, sws, swsb, st))),
         'varifold_gradient': (lambda: ok(lib.lddmm_surface_gradient(0, p(X), n, p(FF), nf, None, p(off), p(items),
@@ -89,8 +91,8 @@ def main():
     XT = torch.stack([X, X])
     AT = A.unsqueeze(0).contiguous()
     PXT = torch.empty_like(XT)
-    calls['fo_adjoint_step'] = (lambda: ok(lib.lddmm_first_order_gradient(p(XT), p(AT), n, 1, s, 1.0, p(P), 1, o,
-                                                                          p(PXT), p(dat), prec, ws, wsb, st)))
+    calls['fo_adjoint_step'] = (lambda: ok(lib.lddmm_first_order_gradient(p(XT), p(AT), n, 1, s, kern, 1.0, p(P), 1,
+                                                                          o, p(PXT), p(dat), prec, ws, wsb, st)))
     pairs = {k: float(n) * n for k in calls}
     pairs['varifold_energy'] = float(nf) * 2 * nf
     pairs['varifold_gradient'] = float(nf) * 2 * nf
@@ -112,10 +114,12 @@ def main():
         ms = e0.elapsed_time(e1) / max(args.reps, 1)
         pps = pairs[name] / (ms * 1e-3)
         fp32, sfu = OPS[name]
-        line = {'op': name, 'level': args.level, 'precision': args.precision, 'ms': round(ms, 4),
-                'pairs_per_s': pps, 'fp32_lane_ops_per_s': pps * fp32,
-                'frac_fp32_peak': pps * fp32 / peak if args.precision == 'fp32' else None,
-                'frac_sfu_peak': pps * sfu / (props.multi_processor_count * 16 * sm_clock * 1e6)}
+        gauss = kern == nat.KERNEL_GAUSS or name.startswith('varifold')   # the op counts are the Gaussian ones
+        line = {'op': name, 'kernel': args.kernel if not name.startswith('varifold') else 'gauss',
+                'level': args.level, 'precision': args.precision, 'ms': round(ms, 4), 'pairs_per_s': pps,
+                'fp32_lane_ops_per_s': pps * fp32 if gauss else None,
+                'frac_fp32_peak': pps * fp32 / peak if args.precision == 'fp32' and gauss else None,
+                'frac_sfu_peak': pps * sfu / (props.multi_processor_count * 16 * sm_clock * 1e6) if gauss else None}
         print(json.dumps(line), flush=True)
 
 

@@ -137,6 +137,45 @@ def shooting_fixtures(kf, evol, shapes, out):
                                   xt=fw['xt'], at=fw['at'], da0=g['da0'], pxt=g['pxt'], pat=g['pat'])
 
 
+def laplacian_fixtures(kf, evol, shapes, out):
+    """The same operators and both shooting variants with the reference's Laplacian kernel
+    (KernelSpec(name='laplacian', order=q), base/kernelFunctions.py:363-368; lap_fun* at
+    base/kernelFunctions_util.py:92-96, 197-203, 239-243, 309-314)."""
+    rng = np.random.default_rng(4321)
+    x, _ = shapes.icosphere(2)
+    n = x.shape[0]
+    y = shapes.bumpy_ellipsoid(x, seed=5)[: n // 3 + 7] * 1.05
+    for order in (1, 3, 4):
+        K = kf.Kernel(name='laplacian', sigma=0.5, order=order)
+        a = rng.normal(size=(n, 3))
+        p = rng.normal(size=(n, 3))
+        q = rng.normal(size=(n, 3))
+        rec = dict(x=x, y=y, a=a, p=p, q=q, sigma=0.5, order=order, regweight=0.7)
+        rec['applyK'] = K.applyK(x, a)
+        rec['applyK_cross'] = K.applyK(x, a, firstVar=y)
+        rec['applyDiffKT'] = K.applyDiffKT(x, p, a)
+        rec['applyDiffKT_cross'] = K.applyDiffKT(x, p[: y.shape[0]], a, firstVar=y)
+        rec['applyDiffKT_sym'] = K.applyDiffKT(x, p, a, sym=True)
+        rec['applyDiffKT_lddmm'] = K.applyDiffKT(x, p, a, lddmm=True, regweight=0.7)
+        rec['applyDDiffK11and12'] = K.applyDDiffK11and12(x, a, q, p)
+        rec['applyDiffK1and2'] = K.applyDiffK1and2(x, p, a)
+        rec['applyDivergence'] = K.applyDivergence(x, a)
+        out[f'laplacian_L2_o{order}'] = rec
+    K = kf.Kernel(name='laplacian', sigma=0.5, order=3)
+    T = 10
+    at = np.stack([smooth_momenta(kf, shapes, x, rng, 0.3, vmax=0.3) for _ in range(T)])
+    px1 = rng.normal(0.0, 0.5, size=x.shape)
+    st = evol.landmarkDirectEvolutionEuler(x, at, K)
+    dat, xt, pxt = evol.landmarkHamiltonianGradient(x, at, px1, K, 0.8, getCovector=True)
+    a0 = smooth_momenta(kf, shapes, x, rng, 0.4, vmax=0.3)
+    fw = evol.secondOrderEvolution(x, a0, K, 0.1)
+    pa1 = rng.normal(0.0, 0.2, size=x.shape)
+    g = evol.secondOrderGradient(x, a0, px1, pa1, K, 0.1)
+    out['laplacian_shooting_L2_o3'] = dict(x0=x, at=at, a0=a0, px1=px1, pa1=pa1, sigma=0.5, order=3, regweight=0.8,
+                                           timeStep=0.1, fo_xt=st['xt'], fo_dat=dat, fo_pxt=pxt, xt=fw['xt'],
+                                           at_so=fw['at'], da0=g['da0'], pxt=g['pxt'], pat=g['pat'])
+
+
 def data_term_fixtures(kf, sd, surf, shapes, out):
     """varifoldNorm0/Def/Gradient, currentNorm0/Def/Gradient, measureNorm0/Def/Gradient
     (base/surfaceDistances.py:22-573)."""
@@ -222,11 +261,13 @@ def main():
     sys.modules['pointset_distances'] = psd
     shapes = load_shapes()
     out = {}
-    only = args.only.split(',') if args.only else ['kernels', 'shooting', 'data', 'matching']
+    only = args.only.split(',') if args.only else ['kernels', 'shooting', 'laplacian', 'data', 'matching']
     if 'kernels' in only:
         kernel_fixtures(kf, shapes, out)
     if 'shooting' in only:
         shooting_fixtures(kf, evol, shapes, out)
+    if 'laplacian' in only:
+        laplacian_fixtures(kf, evol, shapes, out)
     if 'data' in only:
         data_term_fixtures(kf, sd, surf, shapes, out)
     if 'matching' in only:

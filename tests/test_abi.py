@@ -42,9 +42,12 @@ def test_host_only_entry_points():
     assert lib.lddmm_status_string(1) == b'invalid argument'
     # negative sizes and non-positive sigma are rejected before touching the device
     null = ctypes.c_void_p(0)
-    assert lib.lddmm_apply_k(null, -1, null, null, 0, 0.5, None, null, 0, null, 0, null) == 1
-    assert lib.lddmm_apply_k(null, 0, null, null, 0, -0.5, None, null, 0, null, 0, null) == 1
-    assert lib.lddmm_apply_diff_kt(null, 4, null, null, null, 5, 0.5, 2, 1.0, None, null, 0, null, 0, null) == 1
+    assert lib.lddmm_apply_k(null, -1, null, null, 0, 0.5, 0, None, null, 0, null, 0, null) == 1
+    assert lib.lddmm_apply_k(null, 0, null, null, 0, -0.5, 0, None, null, 0, null, 0, null) == 1
+    assert lib.lddmm_apply_k(null, 0, null, null, 0, 0.5, 7, None, null, 0, null, 0, null) == 1     # unknown family
+    assert lib.lddmm_apply_k(null, 0, null, null, 0, 0.5, 21, None, null, 0, null, 0, null) == 1    # order 5
+    assert lib.lddmm_apply_diff_kt(null, 4, null, null, null, 5, 0.5, 0, 2, 1.0, None, null, 0, null, 0, null) == 1
+    assert lib.lddmm_second_order_shoot(null, null, 0, 1, 0.5, 3, 0.1, None, null, null, 0, null, 0, null) == 1
     assert lib.lddmm_workspace_bytes(10, 10, 7) == 0
 
 

@@ -135,7 +135,7 @@ def test_trained_proposal_beats_zero_momentum():
         plain.optimizeMatching()
         warm = SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)),
                                           options=dict(opts))
-        used, obj_prop, obj_zero = lp.warm_start(warm, model)
+        used, obj_prop, obj_zero, _ = lp.warm_start(warm, model)
         assert used and obj_prop < 0.5 * obj_zero, (obj_prop, obj_zero)
         warm.optimizeMatching()
         target = plain.history[-1]

@@ -77,7 +77,7 @@ def test_step_entry_points_match_trajectory():
     ws, wsb = nat.workspace(x0.shape[0], x0.shape[0])
     for t in range(10):
         x1, a1 = torch.empty_like(x), torch.empty_like(a)
-        nat.check(nat.lib().lddmm_second_order_step(nat.ptr(x), nat.ptr(a), x.shape[0], 0.5, 0.1, nat.origin_arg(o),
+        nat.check(nat.lib().lddmm_second_order_step(nat.ptr(x), nat.ptr(a), x.shape[0], 0.5, 0, 0.1, nat.origin_arg(o),
                                                     nat.ptr(x1), nat.ptr(a1), 0, ws, wsb, nat.stream_ptr()))
         x, a = x1, a1
     assert torch.equal(x, xt[-1]) and torch.equal(a, at[-1])
@@ -87,7 +87,7 @@ def test_step_entry_points_match_trajectory():
     for t in range(9, -1, -1):
         p0, q0 = torch.empty_like(px), torch.empty_like(pa)
         nat.check(nat.lib().lddmm_second_order_adjoint_step(nat.ptr(xt[t]), nat.ptr(at[t]), nat.ptr(px), nat.ptr(pa),
-                                                            x.shape[0], 0.5, 0.1, nat.origin_arg(o), nat.ptr(p0),
+                                                            x.shape[0], 0.5, 0, 0.1, nat.origin_arg(o), nat.ptr(p0),
                                                             nat.ptr(q0), 0, ws, wsb, nat.stream_ptr()))
         px, pa = p0, q0
     assert torch.equal(px, pxt[0]) and torch.equal(pa, pat[0])

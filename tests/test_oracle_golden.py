@@ -97,3 +97,54 @@ def test_varifold_weight_gradient_fd():
     fd = (O.varifold_norm_def(xd, F, x1, F, s, weights=w + h * dw)
           - O.varifold_norm_def(xd, F, x1, F, s, weights=w - h * dw)) / (2 * h)
     assert abs(fd - (pxw * dw).sum()) < 1e-6 * max(1.0, abs(fd))
+
+
+LFILES = sorted(glob.glob(os.path.join(GOLDEN, 'laplacian_L2_o*.npz')))
+
+
+@pytest.mark.parametrize('path', LFILES, ids=os.path.basename)
+def test_laplacian_operators(path):
+    """The Laplacian (Matern) kernel of orders 1, 3 and 4 (KernelSpec(name='laplacian', order=q))."""
+    d = np.load(path)
+    s, q = float(d['sigma']), int(d['order'])
+    L = O.laplacian
+    x, y, a, p, qq = d['x'], d['y'], d['a'], d['p'], d['q']
+    ny = y.shape[0]
+    assert rel_err(L.apply_k(x, x, a, s, q), d['applyK']) < TOL
+    assert rel_err(L.apply_k(y, x, a, s, q), d['applyK_cross']) < TOL
+    assert rel_err(L.apply_diff_kt(x, x, p, a, s, order=q), d['applyDiffKT']) < TOL
+    assert rel_err(L.apply_diff_kt(y, x, p[:ny], a, s, order=q), d['applyDiffKT_cross']) < TOL
+    assert rel_err(L.apply_diff_kt(x, x, p, a, s, sym=True, order=q), d['applyDiffKT_sym']) < TOL
+    assert rel_err(L.apply_diff_kt(x, x, p, a, s, lddmm=True, regweight=float(d['regweight']), order=q),
+                   d['applyDiffKT_lddmm']) < TOL
+    assert rel_err(L.apply_ddiff_k11and12(x, a, qq, p, s, q), d['applyDDiffK11and12']) < TOL
+    assert rel_err(L.apply_diff_k1and2(x, p, a, s, q), d['applyDiffK1and2']) < TOL
+    assert rel_err(L.apply_divergence(x, x, a, s, q), d['applyDivergence']) < TOL
+
+
+def test_laplacian_derivative_tables_follow_from_the_kernel():
+    """P1 = (P0 - P0')/u and P2 = (P1 - P1')/u wherever the division is exact (orders >= 1 and >= 2): the tables
+    are the radial derivatives of P0(u) e^-u, the identity the CUDA frame uses to build them."""
+    L = O.laplacian
+    for q in range(5):
+        for src, dst, lo in ((L.P0, L.P1, 1), (L.P1, L.P2, 2)):
+            c = src[q]
+            d = c - np.append(np.arange(1, 5) * c[1:], 0.0)
+            want = np.append(d[1:], 0.0) if q >= lo else np.zeros(5)
+            assert np.abs(want - dst[q]).max() < 1e-15, (q, lo)
+
+
+def test_laplacian_shooting():
+    d = np.load(os.path.join(GOLDEN, 'laplacian_shooting_L2_o3.npz'))
+    s, w, dt = float(d['sigma']), float(d['regweight']), float(d['timeStep'])
+    ops = O.laplacian.ops(int(d['order']))
+    assert rel_err(O.landmark_direct_evolution_euler(d['x0'], d['at'], s, ops), d['fo_xt']) < TOL
+    dat, _, pxt = O.landmark_hamiltonian_gradient(d['x0'], d['at'], d['px1'], s, w, ops)
+    assert rel_err(dat, d['fo_dat']) < TOL
+    assert rel_err(pxt, d['fo_pxt']) < TOL
+    g = O.second_order_gradient(d['x0'], d['a0'], d['px1'], d['pa1'], s, dt, ops)
+    assert rel_err(g['xt'], d['xt']) < TOL
+    assert rel_err(g['at'], d['at_so']) < TOL
+    assert rel_err(g['da0'], d['da0']) < 1e-11
+    assert rel_err(g['pxt'], d['pxt']) < 1e-11
+    assert rel_err(g['pat'], d['pat']) < 1e-11

@@ -29,8 +29,8 @@ def _run(lib, nat, torch, Y, X, A, sigma, static):
                                       nat.ptr(out), nat.FP32C, nat.stream_ptr())
     else:
         ws, wsb = nat.workspace(Y.shape[0], X.shape[0], nat.FP32C)
-        rc = lib.lddmm_apply_k(nat.ptr(Y), Y.shape[0], nat.ptr(X), nat.ptr(A), X.shape[0], sigma, o, nat.ptr(out),
-                               nat.FP32C, ws, wsb, nat.stream_ptr())
+        rc = lib.lddmm_apply_k(nat.ptr(Y), Y.shape[0], nat.ptr(X), nat.ptr(A), X.shape[0], sigma, nat.KERNEL_GAUSS, o,
+                               nat.ptr(out), nat.FP32C, ws, wsb, nat.stream_ptr())
     assert rc == 0, lib.lddmm_status_string(rc)
     torch.cuda.synchronize()
     return out.cpu().numpy()
