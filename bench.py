@@ -19,7 +19,8 @@ numba kernels, all host threads) and prints the same metric with "impl": "refere
 
   registration  (1 GPU) seconds per registration pair to reach 1e-3 relative energy of the FP64 plain optimum on
             the level-6 problem: plain FP64 path, FP32 path, FP32 path + learned warm start (the other half of the
-            headline metric); skipped with --no-registration
+            headline metric), and the level-4 problem run for 50 BFGS iterations on the FP64 path (both matching
+            classes; the case the reference itself runs on the CPU); skipped with --no-registration
 
 Multi-GPU (torchrun): every rank runs the same workload on its own GPU (independent replicas, weak scaling);
 times are the max over ranks; value = pairs of all ranks / that time.
@@ -157,17 +158,23 @@ def ncu_traffic():
         return None
 
 
-def cpu_baseline(x, a, n_targets, threads):
-    """Oracle (numba float64) on a bounded sample: n_targets targets x all sources, both widths."""
+def cpu_baseline(x, a, n_targets, threads, min_seconds=10.0, start=0):
+    """Oracle (numba float64) on a bounded sample: blocks of n_targets targets x all sources x both widths, over
+    successive target blocks from row `start`, until at least `min_seconds` have been measured (one block at least)."""
     import oracle as O
-    y = x[:n_targets]
-    O.apply_k(y[:64], x[:64], a[:64], SIGMAS[0])      # JIT warm-up
-    t0 = time.perf_counter()
-    for s in SIGMAS:
-        O.apply_k(y, x, a, s)
-    dt = time.perf_counter() - t0
-    pairs = len(SIGMAS) * y.shape[0] * x.shape[0]
-    return pairs / dt, dt, pairs
+    O.apply_k(x[:64], x[:64], a[:64], SIGMAS[0])      # JIT warm-up
+    pairs, dt = 0, 0.0
+    start %= x.shape[0]
+    while True:
+        y = x[start:start + n_targets]
+        t0 = time.perf_counter()
+        for s in SIGMAS:
+            O.apply_k(y, x, a, s)
+        dt += time.perf_counter() - t0
+        pairs += len(SIGMAS) * y.shape[0] * x.shape[0]
+        start = (start + n_targets) % x.shape[0]
+        if dt >= min_seconds:
+            return pairs / dt, dt, pairs
 
 
 def run_reference(args, rank, world):
@@ -185,8 +192,8 @@ def run_reference(args, rank, world):
     for _ in range(args.warmup):
         O.apply_k(x[:256], x, a, SIGMAS[0])
     vals = []
-    for _ in range(args.steps):
-        v, dt, pairs = cpu_baseline(x, a, n_t, threads)
+    for step in range(args.steps):
+        v, dt, pairs = cpu_baseline(x, a, n_t, threads, min_seconds=0.0, start=step * n_t)
         vals.append((v, dt, pairs))
     tot_pairs = sum(p for _, _, p in vals)
     tot_t = sum(d for _, d, _ in vals)
@@ -412,13 +419,13 @@ def run_b200(args, rank, world, local_rank):
                 'ms_per_step': float(te) / args.steps, 'api': 'Kernel.applyK(numpy x, numpy a)'},
         'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak_fp32, 'unit': 'T FP32 lane-ops/s',
                      'frac': achieved / peak_fp32, 'sfu_frac': sfu_frac, 'traffic': traffic,
-                     'kernel': 'pairs_kernel<OpK<float>> (+ epilogue, timed together per call)',
+                     'kernel': 'pairs_kernel<OpK, F2, 128, 4, Gauss> + finalize_kernel (timed together per call)',
                      'ops_per_pair': {'fp32': OPS_FP32_PER_PAIR, 'sfu': OPS_SFU_PER_PAIR},
                      'peak_source': f'{n_sm} SMs x 128 FP32 lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
                                     f'max SM clock; MEASURED_PEAKS.json has no FP32 figure)'},
         'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': os.cpu_count(), 'kind': 'port',
-                         'sample': f'{cb_targets} targets x {n} sources x {len(SIGMAS)} widths, float64 numba oracle, '
-                                   f'{cb_dt:.2f} s'},
+                         'sample': f'{cb_pairs:.3g} pairs: blocks of {cb_targets} targets x {n} sources x '
+                                   f'{len(SIGMAS)} widths, float64 numba oracle, {cb_dt:.1f} s'},
         'clocks': clocks, 'gpu_launches': launches,
         'pairs_per_step': pairs_per_step,
     }

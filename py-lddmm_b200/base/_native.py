@@ -68,6 +68,7 @@ _RESTYPES = {'lddmm_version': ctypes.c_char_p, 'lddmm_status_string': ctypes.c_c
 
 _lib = None
 _lock = threading.Lock()
+_PINNED_MIN_BYTES = 1 << 16   # host <-> device copies at least this large go through page-locked staging
 
 
 class LddmmError(RuntimeError):
@@ -174,7 +175,21 @@ def as_device(a, device=None, dtype=torch.float64):
     t = torch.from_numpy(arr)
     if dtype != t.dtype:
         t = t.to(dtype)
+    if t.numel() * t.element_size() >= _PINNED_MIN_BYTES:
+        # staged through page-locked memory (torch's caching host allocator) and copied asynchronously on the
+        # current stream; the staging block is not reused before the copy has completed
+        return t.pin_memory().to(device='cuda' if device is None else device, non_blocking=True)
     return t.to(device='cuda' if device is None else device)
+
+
+def to_host(t):
+    """Device tensor -> new numpy array, read back through page-locked memory for large results."""
+    if t.numel() * t.element_size() < _PINNED_MIN_BYTES:
+        return t.cpu().numpy()
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return h.numpy()
 
 
 def centroid(t):
@@ -182,7 +197,8 @@ def centroid(t):
     device tensors with one reduction (and one synchronisation)."""
     if not isinstance(t, torch.Tensor):
         a = np.asarray(t, dtype=np.float64).reshape(-1, 3)
-        return None if a.size == 0 else a.mean(axis=0).tolist()
+        # ones @ a (one BLAS gemv) instead of a.mean(axis=0), whose strided reduction is ~20x slower for (N,3)
+        return None if a.size == 0 else (np.ones(a.shape[0]) @ a / a.shape[0]).tolist()
     if t.numel() == 0:
         return None
     return t.reshape(-1, 3).mean(dim=0).tolist()

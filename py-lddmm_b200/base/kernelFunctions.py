@@ -31,7 +31,7 @@ def _is_np(v):
 
 
 def _out(t, like_numpy):
-    return t.cpu().numpy() if like_numpy else t
+    return nat.to_host(t) if like_numpy else t
 
 
 class KernelSpec:
