@@ -6,21 +6,22 @@ when the proposal does not lower the objective (`warm_start`).
 
 Features per source vertex (all computed on the device by the library's kernels):
   centred position (3), area-weighted vertex normal (3), nearest-target displacement d (3), its kernel-smoothed
-  versions sum_l K(x_k,x_l) d_l / sum_l K(x_k,x_l) at widths 0.25 and 0.5 (6, the kernel-smoothed aggregation over
-  the surface), normal component d.n (1), |d| (1) -> 17, zero-padded to 64 (the GEMM tile width).
+  versions sum_l K(x_k,x_l) d_l / sum_l K(x_k,x_l) at widths 0.25 and 0.5 (6), normal component d.n (1), |d| (1),
+  and the normalised kernel smoothings of d.n and |d| at widths 0.1, 0.2, 0.35 and 0.7 (8, the kernel-smoothed
+  aggregation over the surface) -> 25, zero-padded to 64 (the GEMM tile width).
 Network: 64 -> 128 -> 128 -> 128 -> 64 (outputs 0..2 used), ReLU, BF16 weights and activations, FP32 accumulation
 and FP32 master weights (Adam), all GEMMs in `lddmm_bf16_gemm` (mma.sync tensor cores).
-Output: the normal component (v0.n) n of the initial velocity v0 = K(x0) a0, over VELOCITY_SCALE. The velocity is a
-smooth, resolution-independent field (the raw momentum, a kernel inverse of it, is not), and only its normal part
-is determined by the target shape: tangential motion leaves the surface unchanged, is invisible to any shape
-feature and is left to the regulariser during refinement. The momentum proposal is recovered by a normalised kernel
-inverse: the predicted velocity is smoothed (sum K_0.25 v / sum K_0.25) and divided by the kernel mass
-sum_l K(x_k, x_l) of the deformation kernel, which inverts K for fields smooth at its width and applies unchanged at
-any mesh resolution.
+Output: the momentum density m = a0 * mass (N,3), mass_k = sum_l K(x_k, x_l) the kernel mass of the deformation
+kernel, over MOMENTUM_SCALE. The density has velocity units and does not depend on the mesh resolution (the momentum
+itself is a discrete measure that scales with 1/mass), so a network trained at one level applies at any other; the
+proposal is a0 = m / mass. Predicting the momentum (a deconvolution of the displacement, which the multi-scale
+features give the network) rather than the velocity K a0 matters: started from the exact normal velocity turned
+into a momentum by the normalised kernel inverse, BFGS needs as many iterations as from the network's velocity,
+three times more than from the exact momentum.
 
 Training data: pairs generated by the method itself -- random smooth normal momentum fields a = (K_s z) n (z a
 scalar white-noise field, rescaled to an initial speed drawn in [vmin, vmax]) shot with the deformation kernel; the
-label is the normal part of the generating initial velocity.
+label is the momentum density of the generating momentum.
 """
 import math
 
@@ -32,8 +33,9 @@ from . import pointEvolution as evol
 from .kernelFunctions import Kernel
 
 IN_DIM, HIDDEN, OUT_DIM, N_OUT = 64, 128, 64, 3
-N_FEATURES = 17
-VELOCITY_SCALE = 0.3
+N_FEATURES = 25
+MOMENTUM_SCALE = 0.3
+SCALAR_WIDTHS = (0.1, 0.2, 0.35, 0.7)
 ROW_PAD = 64
 
 
@@ -76,33 +78,25 @@ def pair_features(X0, faces_t, X1, normals=None):
     nrm = vertex_normals(X0, faces_t) if normals is None else normals
     d = nearest_displacement(X0, X1)
     ones = torch.ones_like(X0)
+    dn = (d * nrm).sum(dim=1, keepdim=True)
+    dl = d.norm(dim=1, keepdim=True)
     feats = [X0 - X0.mean(dim=0, keepdim=True), nrm, d]
     for s in (0.25, 0.5):
         K = _smoother(s)
         feats.append(K.applyK(X0, d) / K.applyK(X0, ones))
-    feats.append((d * nrm).sum(dim=1, keepdim=True))
-    feats.append(d.norm(dim=1, keepdim=True))
+    feats += [dn, dl]
+    scal = torch.cat([dn, dl, torch.ones_like(dn)], dim=1).contiguous()   # one kernel sum smooths both and the mass
+    for s in SCALAR_WIDTHS:
+        r = _smoother(s).applyK(X0, scal)
+        feats.append(r[:, :2] / r[:, 2:3])
     F = torch.zeros((_pad_rows(n), IN_DIM), dtype=torch.bfloat16, device=X0.device)
     F[:n, :N_FEATURES] = torch.cat(feats, dim=1).to(torch.bfloat16)
     return F
 
 
-def kernel_cg(K, X, b, a0, iters):
-    """`iters` conjugate-gradient steps on K(X) a = b from a0 (K symmetric positive definite); every product is one
-    kernel sum in the library, the scalars stay on the device (no host synchronisation)."""
-    a = a0.clone()
-    r = b - K.applyK(X, a)
-    p = r.clone()
-    rr = (r * r).sum()
-    for _ in range(iters):
-        q = K.applyK(X, p)
-        alpha = rr / (p * q).sum().clamp_min(1e-300)
-        a = a + alpha * p
-        r = r - alpha * q
-        rr_new = (r * r).sum()
-        p = r + (rr_new / rr.clamp_min(1e-300)) * p
-        rr = rr_new
-    return a
+def kernel_mass(K, X):
+    """mass_k = sum_l K(x_k, x_l) (N,1)."""
+    return K.applyK(X, torch.ones_like(X))[:, :1]
 
 
 class MomentumProposal:
@@ -188,25 +182,16 @@ class MomentumProposal:
                                                 weight_decay, nat.stream_ptr()), 'adam_step')
 
     # ------------------------------------------------------------------ inference
-    def predict_velocity(self, X0, faces_t, X1, normals=None):
-        """Predicted initial velocity v0 (N,3) f64 for registering X0 (with faces) onto the target points X1."""
+    def predict_density(self, X0, faces_t, X1, normals=None):
+        """Predicted momentum density m = a0 * mass (N,3) f64 for registering X0 (with faces) onto X1."""
         n = X0.shape[0]
         F = pair_features(X0, faces_t, X1, normals)
         y = self.forward(F)
-        return (y[:n, :N_OUT].to(torch.float64) * VELOCITY_SCALE).contiguous()
+        return (y[:n, :N_OUT].to(torch.float64) * MOMENTUM_SCALE).contiguous()
 
-    def predict(self, X0, faces_t, X1, Kdef, normals=None, cg_iters=0):
-        """Initial momentum proposal a0 (N,3) f64: the smoothed predicted velocity v divided by the kernel mass of
-        Kdef, optionally refined by `cg_iters` conjugate-gradient steps on K(x0) a = v (early stopping keeps the
-        kernel inverse from amplifying the prediction's vertex-level noise)."""
-        v = self.predict_velocity(X0, faces_t, X1, normals)
-        ones = torch.ones_like(X0)
-        Ks = _smoother(0.25)
-        v = Ks.applyK(X0, v) / Ks.applyK(X0, ones)
-        a = v / Kdef.applyK(X0, ones)
-        if cg_iters > 0:
-            a = kernel_cg(Kdef, X0, v, a, cg_iters)
-        return a.contiguous()
+    def predict(self, X0, faces_t, X1, Kdef, normals=None):
+        """Initial momentum proposal a0 (N,3) f64: the predicted density divided by the kernel mass of Kdef."""
+        return (self.predict_density(X0, faces_t, X1, normals) / kernel_mass(Kdef, X0)).contiguous()
 
     def state_dict(self):
         return {'W': [w.cpu() for w in self.W], 'b': [b.cpu() for b in self.b], 'step': self.step}
@@ -226,8 +211,8 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     (x0, shoot(x0, a_i)).
 
     a_i = (K_{sigma_smooth} z) n with z a scalar white-noise field, rescaled to an initial speed ~ U[vmin, vmax];
-    targets shot with K_{sigma_def} over round(1/timeStep) steps; labels are the normal parts of the initial
-    velocities K_{sigma_def}(x0) a_i, over VELOCITY_SCALE."""
+    targets shot with K_{sigma_def} over round(1/timeStep) steps; labels are the momentum densities a_i * mass
+    (mass of K_{sigma_def}), over MOMENTUM_SCALE."""
     X0 = nat.as_device(x0)
     faces_t = torch.from_numpy(np.ascontiguousarray(faces, dtype=np.int64)).cuda()
     n = X0.shape[0]
@@ -243,16 +228,15 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     labels = torch.zeros((n_pairs, Mp, N_OUT), dtype=torch.float32, device='cuda')
     momenta = torch.zeros((n_pairs, n, 3), dtype=torch.float64, device='cuda')
     origin = nat.centroid(X0)
+    mass = kernel_mass(Kdef, X0)
     for i in range(n_pairs):
         z = torch.randn((n, 1), generator=gen, dtype=torch.float64, device='cuda').expand(n, 3).contiguous()
         a = Ksm.applyK(X0, z)[:, :1] * normals
         v = Kdef.applyK(X0, a)
-        scale = speeds[i] / v.norm(dim=1).max()
-        a, v = a * scale, v * scale
+        a = a * (speeds[i] / v.norm(dim=1).max())
         xt, _ = evol.shoot_second_order(X0, a, Kdef, timeStep, origin=origin)
         feats[i] = pair_features(X0, faces_t, xt[-1], normals)
-        vn = (v * normals).sum(dim=1, keepdim=True) * normals
-        labels[i, :n] = (vn / VELOCITY_SCALE).to(torch.float32)
+        labels[i, :n] = (a * mass / MOMENTUM_SCALE).to(torch.float32)
         momenta[i] = a
     return feats, labels, momenta, n
 
@@ -281,14 +265,14 @@ def train(model, feats, labels, n, epochs=10, batch_pairs=16, lr=1e-3, seed=0, l
     return history
 
 
-def warm_start(matching, model, cg_iters=0, scales=(1.0,)):
+def warm_start(matching, model, scales=(1.0,)):
     """Set matching.control['a0'] to the network's proposal when it lowers the objective, else keep zero momentum
     (the plain optimiser is the fallback). With several `scales`, the proposal is tried at each multiple and the
     best one is kept (one forward shot per scale). Returns (used_proposal, objective_at_proposal, objective_at_zero,
     chosen_scale)."""
     X0 = matching.x0
     faces_t = matching.data.faces
-    a_prop = model.predict(X0, faces_t, matching.data.x1, matching.options['KparDiff'], cg_iters=cg_iters)
+    a_prop = model.predict(X0, faces_t, matching.data.x1, matching.options['KparDiff'])
     zero = torch.zeros_like(a_prop)
     matching.obj = None
     obj_zero = matching.objectiveFun() if torch.equal(matching.control['a0'], zero) else None

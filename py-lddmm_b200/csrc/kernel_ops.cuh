@@ -124,10 +124,10 @@ struct OpDiffKT {
 
 // DDK_{11 and 12}(x; n, a, p) -- base/kernelFunctions_util.py:1091-1129 ('11and12'), gauss_fun_ddiff (:299).
 // out_k = sum_l (n_k.a_l) e [ (D.Dp) D / sigma^4 - Dp / sigma^2 ],  D = x_k - x_l, Dp = p_k - p_l
-//       = kappa^2 A_k - (p_k B_k - C_k)/sigma^2 with A = sum c e (d.Dp) d, B = sum c e, C = sum c e p_l.
-// 24 FP32 + 1 SFU per pair.
+//       = kappa^2 A_k - B_k / sigma^2 with A = sum c e (d.Dp) d, B = sum c e Dp (c = n_k.a_l).
+// 23 FP32 + 1 SFU per pair (the Dp components are shared by d.Dp and B).
 struct OpDDiffK {
-  static constexpr int NS = 9, NA = 7;
+  static constexpr int NS = 9, NA = 6;
   struct Params {
     const double *x, *nn, *a, *p;
     double* out;
@@ -157,22 +157,21 @@ struct OpDDiffK {
   static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
     const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
-    const V dq = dot3(d0, d1, d2, t.p0 - s[6], t.p1 - s[7], t.p2 - s[8]);
+    const V q0 = t.p0 - s[6], q1 = t.p1 - s[7], q2 = t.p2 - s[8];
+    const V dq = dot3(d0, d1, d2, q0, q1, q2);
     const V na = dot3(t.n0, t.n1, t.n2, s[3], s[4], s[5]);
     const V ce = k.k1 * na;
     const V ced = (k.k2 * na) * dq;  // == ce * dq for the Gaussian
     acc[0] = fma(ced, d0, acc[0]);
     acc[1] = fma(ced, d1, acc[1]);
     acc[2] = fma(ced, d2, acc[2]);
-    acc[3] = acc[3] + ce;
-    acc[4] = fma(ce, s[6], acc[4]);
-    acc[5] = fma(ce, s[7], acc[5]);
-    acc[6] = fma(ce, s[8], acc[6]);
+    acc[3] = fma(ce, q0, acc[3]);
+    acc[4] = fma(ce, q1, acc[4]);
+    acc[5] = fma(ce, q2, acc[5]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k2 = P.f.kappa * P.f.kappa, is2 = P.f.inv_s2;
-    for (int c = 0; c < 3; ++c)
-      P.out[3 * i + c] = k2 * acc[c] - is2 * (P.p[3 * i + c] * acc[3] - acc[4 + c]);
+    for (int c = 0; c < 3; ++c) P.out[3 * i + c] = k2 * acc[c] - is2 * acc[3 + c];
   }
 };
 

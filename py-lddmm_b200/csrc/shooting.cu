@@ -63,13 +63,13 @@ struct OpSOFwd {
 //   px_prev = px + dt zpx,  pa_prev = pa + dt zpa.
 // With c1' = px'_k.a_l + a_k.px'_l (px' = -kappa px), c2'' = a''_k.a_l (a'' = -kappa^2 a), dq = d.(pa_k - pa_l)
 // the accumulators are
-//   G = sum e (c1' + c2'' dq) d (3), C = sum e c2'' (1), D = sum e c2'' pa_l (3), E = sum e px'_l (3),
-//   F = sum e dq a_l (3)
-// and zpx = G + (pa_k C - D)/(sigma^2 (-kappa^2)), zpa = E/(-kappa) + kappa F. 38 FP32 + 1 SFU per pair.
+//   G = sum e (c1' + c2'' dq) d (3), D = sum e c2'' (pa_k - pa_l) (3), E = sum e px'_l (3), F = sum e dq a_l (3)
+// and zpx = G + D/(sigma^2 (-kappa^2)), zpa = E/(-kappa) + kappa F. 37 FP32 + 1 SFU per pair (the pa_k - pa_l
+// components are shared by dq and D).
 // Targets are rows row0 .. row0+n-1 of the state and covectors (row0 = 0 for a whole step), sources all rows;
 // outputs px_prev, pa_prev are indexed by the local target index.
 struct OpSOBwd {
-  static constexpr int NS = 12, NA = 13;
+  static constexpr int NS = 12, NA = 12;
   struct Params {
     const double *x, *a, *px, *pa;
     double *px_prev, *pa_prev;
@@ -113,7 +113,8 @@ struct OpSOBwd {
   static __device__ __forceinline__ void pair(const Frame& f, const Tgt<V>& t, const V* s, V* acc) {
     const V d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
     const KV<V> k = Fam::template eval<V>(f, sqdist(d0, d1, d2));
-    const V dq = dot3(d0, d1, d2, t.q0 - s[6], t.q1 - s[7], t.q2 - s[8]);
+    const V w0 = t.q0 - s[6], w1 = t.q1 - s[7], w2 = t.q2 - s[8];
+    const V dq = dot3(d0, d1, d2, w0, w1, w2);
     const V c1 = fma(t.a2, s[11], fma(t.a1, s[10], fma(t.a0, s[9], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
     const V c2 = dot3(t.b0, t.b1, t.b2, s[3], s[4], s[5]);
     const V ec2 = k.k1 * c2;
@@ -121,17 +122,16 @@ struct OpSOBwd {
     acc[0] = fma(eg, d0, acc[0]);
     acc[1] = fma(eg, d1, acc[1]);
     acc[2] = fma(eg, d2, acc[2]);
-    acc[3] = acc[3] + ec2;
-    acc[4] = fma(ec2, s[6], acc[4]);
-    acc[5] = fma(ec2, s[7], acc[5]);
-    acc[6] = fma(ec2, s[8], acc[6]);
-    acc[7] = fma(k.k0, s[9], acc[7]);
-    acc[8] = fma(k.k0, s[10], acc[8]);
-    acc[9] = fma(k.k0, s[11], acc[9]);
+    acc[3] = fma(ec2, w0, acc[3]);
+    acc[4] = fma(ec2, w1, acc[4]);
+    acc[5] = fma(ec2, w2, acc[5]);
+    acc[6] = fma(k.k0, s[9], acc[6]);
+    acc[7] = fma(k.k0, s[10], acc[7]);
+    acc[8] = fma(k.k0, s[11], acc[8]);
     const V edq = k.k1 * dq;
-    acc[10] = fma(edq, s[3], acc[10]);
-    acc[11] = fma(edq, s[4], acc[11]);
-    acc[12] = fma(edq, s[5], acc[12]);
+    acc[9] = fma(edq, s[3], acc[9]);
+    acc[10] = fma(edq, s[4], acc[10]);
+    acc[11] = fma(edq, s[5], acc[11]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double k = P.f.kappa;
@@ -139,8 +139,8 @@ struct OpSOBwd {
     const int g = P.row0 + i;
     for (int c = 0; c < 3; ++c) {
       const double pa = P.pa[3 * g + c];
-      const double zpx = acc[c] + cd * (pa * acc[3] - acc[4 + c]);
-      const double zpa = -acc[7 + c] / k + k * acc[10 + c];
+      const double zpx = acc[c] + cd * acc[3 + c];
+      const double zpa = -acc[6 + c] / k + k * acc[9 + c];
       P.px_prev[3 * i + c] = P.px[3 * g + c] + P.dt * zpx;
       P.pa_prev[3 * i + c] = pa + P.dt * zpa;
     }

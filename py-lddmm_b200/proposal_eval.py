@@ -37,12 +37,12 @@ from base.syntheticShapes import icosphere  # noqa: E402
 
 
 def register(x0, F, x1, dtype, target=None, model=None, maxIter=1000, sigma=0.5, sigma_dist=0.3, time_step=0.1,
-             scales=(1.0,)):
+             scales=(1.0,), a0=None):
     K = Kernel(name='gauss', sigma=sigma)
     K.pk_dtype = dtype
     opts = dict(maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=K, KparDist=('gauss', sigma_dist),
                 sigmaError=1.0, errorType='varifold', pk_dtype=dtype, algorithm='bfgs', timeStep=time_step,
-                verb=False, targetObjective=target)
+                verb=False, targetObjective=target, initialMomentum=a0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     f = SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
@@ -71,6 +71,8 @@ def main():
     ap.add_argument('--scales', default='1.0;0.25,0.5,0.75,1.0',
                     help="learned variants separated by ';', each a comma-separated list of multiples of the proposal "
                          "tried at the start (the best one is kept)")
+    ap.add_argument('--true-momentum', action='store_true',
+                    help='also start BFGS from the momentum that generated the pair (the best a proposal could know)')
     ap.add_argument('--verbose', action='store_true')
     args = ap.parse_args()
     variants = [tuple(float(v) for v in grp.split(',')) for grp in args.scales.split(';')]
@@ -112,6 +114,9 @@ def main():
             row.update({f'learned{v}_iters': len(fl.history), f'learned{v}_s': sl,
                         f'learned{v}_reached': bool(fl.reached_target), f'learned{v}_used': used[0],
                         f'learned{v}_obj_ratio': used[1] / used[2], f'learned{v}_scale': used[3]})
+        if args.true_momentum:
+            ft, _, st_, _ = register(x0, F, x1, 'float32', target=target, a0=momenta[i].cpu().numpy())
+            row.update({'true_iters': len(ft.history), 'true_s': st_, 'true_reached': bool(ft.reached_target)})
         rows.append(row)
         if args.verbose:
             print(json.dumps(row), flush=True)
@@ -123,7 +128,7 @@ def main():
     summary = {'experiment': 'learned proposal, held-out shot pairs', 'level': args.level, 'vertices': int(n),
                'pairs': args.pairs, 'trained_on': ntr, 'heldout': args.heldout, 'evaluated': len(rows),
                'epochs': args.epochs, 'generate_s': gen_s, 'train_s': train_s,
-               'loss_first_last': [hist[0], hist[-1]], 'heldout_velocity_rel_err': vel_err, 'tol': args.tol,
+               'loss_first_last': [hist[0], hist[-1]], 'heldout_label_rel_err': vel_err, 'tol': args.tol,
                'fp64_plain_iters_to_tol': stats('fp64_iters_to_tol'), 'fp64_plain_s_to_tol': stats('fp64_s_to_tol'),
                'fp32_plain_iters': stats('fp32_iters'), 'fp32_plain_s': stats('fp32_s'),
                'fp32_plain_all_reached': all(r['fp32_reached'] for r in rows)}
@@ -132,6 +137,9 @@ def main():
                                   'used_frac': sum(r[f'learned{v}_used'] for r in rows) / max(len(rows), 1),
                                   'obj_proposal_over_zero': stats(f'learned{v}_obj_ratio'),
                                   'all_reached': all(r[f'learned{v}_reached'] for r in rows)}
+    if args.true_momentum:
+        summary['true_momentum_start'] = {'iters': stats('true_iters'), 's': stats('true_s'),
+                                          'all_reached': all(r['true_reached'] for r in rows)}
     print(json.dumps(summary), flush=True)
 
 
