@@ -239,7 +239,7 @@ def run_registration(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         f = SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
-        used = lp.warm_start(f, model) if model is not None else None
+        used = lp.warm_start(f, model, scales=(0.5, 0.75, 1.0)) if model is not None else None
         f.optimizeMatching()
         torch.cuda.synchronize()
         return f, time.perf_counter() - t0, used

@@ -210,7 +210,8 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     """Features (n_pairs, Mpad, IN_DIM) bf16, labels (n_pairs, Mpad, 3) f32 and momenta (n_pairs, n, 3) f64 of pairs
     (x0, shoot(x0, a_i)).
 
-    a_i = (K_{sigma_smooth} z) n with z a scalar white-noise field, rescaled to an initial speed ~ U[vmin, vmax];
+    a_i = (K_{sigma_smooth} z) n with z a scalar white-noise field, rescaled to an initial speed ~ U[vmin, vmax]
+    (several widths: a sum of such fields, one per width, with random weights U[0, 1]);
     targets shot with K_{sigma_def} over round(1/timeStep) steps; labels are the momentum densities a_i * mass
     (mass of K_{sigma_def}), over MOMENTUM_SCALE."""
     X0 = nat.as_device(x0)
@@ -219,8 +220,12 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     Mp = _pad_rows(n)
     Kdef = Kernel(name='gauss', sigma=sigma_def)
     Kdef.pk_dtype = 'float32'
-    Ksm = Kernel(name='gauss', sigma=sigma_smooth)
-    Ksm.pk_dtype = 'float32'
+    widths = tuple(sigma_smooth) if isinstance(sigma_smooth, (tuple, list)) else (sigma_smooth,)
+    Ksm = []
+    for w in widths:
+        k = Kernel(name='gauss', sigma=w)
+        k.pk_dtype = 'float32'
+        Ksm.append(k)
     normals = vertex_normals(X0, faces_t)
     gen = torch.Generator(device='cuda').manual_seed(seed)
     speeds = torch.rand(n_pairs, generator=gen, dtype=torch.float64, device='cuda') * (vmax - vmin) + vmin
@@ -230,8 +235,12 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     origin = nat.centroid(X0)
     mass = kernel_mass(Kdef, X0)
     for i in range(n_pairs):
-        z = torch.randn((n, 1), generator=gen, dtype=torch.float64, device='cuda').expand(n, 3).contiguous()
-        a = Ksm.applyK(X0, z)[:, :1] * normals
+        a = torch.zeros_like(X0)
+        for k in Ksm:
+            z = torch.randn((n, 1), generator=gen, dtype=torch.float64, device='cuda').expand(n, 3).contiguous()
+            f = k.applyK(X0, z)[:, :1]
+            wt = torch.rand((), generator=gen, dtype=torch.float64, device='cuda') if len(Ksm) > 1 else 1.0
+            a = a + wt * f / f.abs().max() * normals
         v = Kdef.applyK(X0, a)
         a = a * (speeds[i] / v.norm(dim=1).max())
         xt, _ = evol.shoot_second_order(X0, a, Kdef, timeStep, origin=origin)
