@@ -31,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -71,7 +72,9 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.t0 = self.t1 = None
-        self.path = os.path.join(REPO, 'gpurun_out', f'clocks_rank{device_index}.csv')
+        # raw samples: $LDDMM_CLOCK_LOG (a directory) if set, else the system temporary directory
+        base = os.environ.get('LDDMM_CLOCK_LOG') or tempfile.gettempdir()
+        self.path = os.path.join(base, f'clocks_rank{device_index}.csv')
 
     def _gpu_id(self):
         try:
