@@ -11,7 +11,9 @@ import numpy as np
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), 'lib', 'liblddmm_b200.so')
+# the in-tree build; LDDMM_B200_LIB names another build of the same library (e.g. one compiled with other tuning
+# macros) to load instead
+LIB_PATH = os.environ.get('LDDMM_B200_LIB') or os.path.join(os.path.dirname(_HERE), 'lib', 'liblddmm_b200.so')
 
 FP32C = 0
 FP64 = 1

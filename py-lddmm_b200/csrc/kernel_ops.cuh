@@ -23,6 +23,7 @@ __device__ __forceinline__ V dot3(V a0, V a1, V a2, V b0, V b1, V b2) {
 // dots[i] = dotw_i . (K a)_i for FP64 energy reductions.
 struct OpK {
   static constexpr int NS = 6, NA = 3;
+  static constexpr bool kCompInRegisters = true;  // measured faster than shared memory for this op
   struct Params {
     const double *y, *x, *a;
     double* out;
@@ -128,6 +129,7 @@ struct OpDiffKT {
 // 23 FP32 + 1 SFU per pair (the Dp components are shared by d.Dp and B).
 struct OpDDiffK {
   static constexpr int NS = 9, NA = 6;
+  static constexpr bool kCompInRegisters = true;  // measured faster than shared memory for this op
   struct Params {
     const double *x, *nn, *a, *p;
     double* out;

@@ -22,8 +22,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #ifndef LDDMM_MIN_CTAS
 #define LDDMM_MIN_CTAS 1  // minimum resident CTAs per SM requested from ptxas (caps registers when > 1)
+#endif
+#ifndef LDDMM_COMP_SMEM
+#define LDDMM_COMP_SMEM 1  // 0: keep every op's compensated (hi, lo) sums in registers
 #endif
 #ifndef LDDMM_SOURCE_UNROLL
 #define LDDMM_SOURCE_UNROLL 4  // unroll depth of the per-source loop over a shared-memory tile
@@ -126,8 +131,13 @@ template <> struct VT<double> {
 // Compensated accumulator: a tile sum `t` is folded into (hi, lo) by Knuth's two-sum (FP32); plain sum (FP64).
 template <typename V> struct Comp;
 template <> struct Comp<F2> {
+  static constexpr int kWords = 2;  // (hi, lo)
   F2 hi, lo;
   __device__ __forceinline__ void zero() { hi = lo = f2(0.f, 0.f); }
+  template <int TPB>
+  __device__ __forceinline__ void load(const F2 (*cs)[TPB], int i, int t) { hi = cs[2 * i][t]; lo = cs[2 * i + 1][t]; }
+  template <int TPB>
+  __device__ __forceinline__ void store(F2 (*cs)[TPB], int i, int t) const { cs[2 * i][t] = hi; cs[2 * i + 1][t] = lo; }
   __device__ __forceinline__ void merge(F2 t) {
     const F2 s = hi + t;
     const F2 bp = s - hi;
@@ -140,11 +150,23 @@ template <> struct Comp<F2> {
   }
 };
 template <> struct Comp<double> {
+  static constexpr int kWords = 1;
   double hi;
   __device__ __forceinline__ void zero() { hi = 0.0; }
+  template <int TPB>
+  __device__ __forceinline__ void load(const double (*cs)[TPB], int i, int t) { hi = cs[i][t]; }
+  template <int TPB>
+  __device__ __forceinline__ void store(double (*cs)[TPB], int i, int t) const { cs[i][t] = hi; }
   __device__ __forceinline__ void merge(double t) { hi += t; }
   __device__ __forceinline__ double partial(int) const { return hi; }
 };
+
+// Ops whose compensated sums stay in registers (few accumulators: measured faster there) declare
+// `static constexpr bool kCompInRegisters = true;`.
+template <class Op, class = void>
+struct CompInRegisters : std::false_type {};
+template <class Op>
+struct CompInRegisters<Op, std::void_t<decltype(Op::kCompInRegisters)>> : std::bool_constant<Op::kCompInRegisters> {};
 
 __device__ __forceinline__ double partial_value(float2 p) { return (double)p.x + (double)p.y; }
 __device__ __forceinline__ double partial_value(double p) { return p; }
@@ -303,6 +325,10 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
   constexpr int NU = (Op::NS + 1) / 2;
   static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
   __shared__ Unit<V> sm[NU][TPB];
+  // The segment's compensated sums live in shared memory (one private column per thread: no barrier needed) unless
+  // the op keeps them in registers; shared memory frees 2-4 registers per accumulator for more resident warps.
+  constexpr bool kSm = LDDMM_COMP_SMEM && !CompInRegisters<Op>::value;
+  __shared__ V cs[kSm ? G * Op::NA * Comp<V>::kWords : 1][TPB];
 
   const long long u_end = sk_start(blockIdx.x + 1, W, C);
   long long u = sk_start(blockIdx.x, W, C);
@@ -313,7 +339,7 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
     const int slot = (int)blockIdx.x - sk_cta_of((long long)tb * TT, W, C);
 
     typename Op::template Tgt<V> tgt[G];
-    Comp<V> cmp[G][Op::NA];
+    Comp<V> cmp[G][Op::NA];   // used when !kSm
     // target of (group g, lane k): base + (g * L + k) * TPB
     const int base = tb * (TPB * RT) + threadIdx.x;
 #pragma unroll
@@ -323,7 +349,10 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
       i1 = i1 < n ? i1 : n - 1;
       Op::template load_target<V>(P, i0, i1, tgt[g]);
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) cmp[g][c].zero();
+      for (int c = 0; c < Op::NA; ++c) {
+        cmp[g][c].zero();
+        if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
+      }
     }
 
     for (int j = j0; j < j1; ++j) {
@@ -362,7 +391,11 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
 #pragma unroll
       for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int c = 0; c < Op::NA; ++c) cmp[g][c].merge(acc[g][c]);
+        for (int c = 0; c < Op::NA; ++c) {
+          if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * Op::NA + c, threadIdx.x);
+          cmp[g][c].merge(acc[g][c]);
+          if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
+        }
       __syncthreads();
     }
 
@@ -373,8 +406,10 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
         const int i = base + (g * L + k) * TPB;
         if (i < n) {
 #pragma unroll
-          for (int c = 0; c < Op::NA; ++c)
+          for (int c = 0; c < Op::NA; ++c) {
+            if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * Op::NA + c, threadIdx.x);
             ws[((size_t)slot * Op::NA + c) * (size_t)n + i] = cmp[g][c].partial(k);
+          }
         }
       }
     u += j1 - j0;

@@ -154,6 +154,7 @@ struct OpSOBwd {
 // Accumulators: A = sum e c d (3), Q = sum e q_l (3). 19 FP32 + 1 SFU per pair.
 struct OpFOBwd {
   static constexpr int NS = 9, NA = 6;
+  static constexpr bool kCompInRegisters = true;  // measured faster than shared memory for this op
   struct Params {
     const double *x, *a, *p;
     double *p_prev, *dat;
