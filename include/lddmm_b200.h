@@ -5,7 +5,8 @@
  *  - Arrays are float64, C-contiguous, on the CUDA device of `stream` (device pointers), in the reference's
  *    layout: points / momenta / covectors are (N, 3) row-major (numpy `float64 (N,3)`), trajectories are
  *    (T+1, N, 3), faces are int64 (F, 3). Outputs are written, never accumulated into, and never alias inputs.
- *  - Gaussian kernel of one width `sigma` with the reference's default `ms_exponent = -1` weighting.
+ *  - One kernel width `sigma` per call (Gaussian, or the Laplacian family where an entry point takes `kernel`),
+ *    with the reference's default `ms_exponent = -1` weighting; multi-scale kernels are one call per width.
  *  - `origin` (host pointer to 3 doubles, may be NULL = 0): coordinates are centred on it before the FP32
  *    conversion. Results are translation invariant; pass the centroid of the points for best FP32 accuracy.
  *  - `precision`: LDDMM_FP32C = FP32 pair arithmetic with compensated (two-sum) accumulation across tiles and
@@ -31,7 +32,8 @@ enum {
   LDDMM_OK = 0,
   LDDMM_ERR_INVALID_ARGUMENT = 1,
   LDDMM_ERR_LAUNCH = 2,
-  LDDMM_ERR_NONFINITE = 3,
+  LDDMM_ERR_NONFINITE = 3, /* reserved: entry points never read results back, so NaN / Inf propagate to the
+                               outputs as in the reference */
   LDDMM_ERR_WORKSPACE = 4,
   LDDMM_ERR_CUDA = 5,
   LDDMM_ERR_UNSUPPORTED = 6

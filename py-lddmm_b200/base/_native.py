@@ -133,10 +133,13 @@ def origin_arg(origin):
 
 
 class Workspace:
-    """Per-device scratch buffer grown on demand (torch caching allocator; never freed while in use)."""
+    """Per-device scratch buffer grown on demand (torch caching allocator). A buffer that is outgrown is retired,
+    not freed: a caller that took its pointer before another request grew the workspace keeps valid memory (the
+    retired buffers add up to less than the current one, sizes being powers of two)."""
 
     def __init__(self):
         self._bufs = {}
+        self._retired = {}
 
     def get(self, nbytes, device=None):
         dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
@@ -144,6 +147,8 @@ class Workspace:
         if buf is None or buf.numel() < nbytes:
             size = max(int(nbytes), 1 << 20)
             size = 1 << (size - 1).bit_length()
+            if buf is not None:
+                self._retired.setdefault(dev.index, []).append(buf)
             buf = torch.empty(size, dtype=torch.uint8, device=dev)
             self._bufs[dev.index] = buf
         return buf
