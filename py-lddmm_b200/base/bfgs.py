@@ -12,6 +12,7 @@ import time
 from copy import deepcopy
 
 import numpy as np
+import torch
 
 from .linesearch import line_search_wolfe, line_search_weak_wolfe, line_search_goldstein_price
 
@@ -29,6 +30,8 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
     line_search = {'Wolfe': line_search_wolfe, 'Goldstein_Price': line_search_goldstein_price,
                    'Weak_Wolfe': line_search_weak_wolfe}.get(lineSearch, line_search_weak_wolfe)
     dot = getattr(opt, 'dotProduct_euclidean', None) or getattr(opt, 'dotProduct', None) or _dot
+    # optional: (u, v) -> u.v as a device scalar, used by the two-loop recursion (no host synchronisation)
+    dot_dev = getattr(opt, 'dotProduct_device', None)
     addProd = getattr(opt, 'addProd', lambda x, y, a: x + a * y)
     prod = getattr(opt, 'prod', lambda x, a: a * x)
     copyDir = getattr(opt, 'copyDir', deepcopy)
@@ -92,20 +95,24 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
             if len(history) > memory:
                 history.pop(0)
             q = copyDir(grd)
+            # the two-loop recursion; with `dot_dev` (device scalars) it runs without reading anything back
+            d = dot_dev or (lambda u, v: dot(u, [v])[0])
             rho, alpha = [], []
             for s_k, y_k in reversed(history):
-                rho.append(1 / dot(y_k, [s_k])[0])
-                alpha.append(rho[-1] * dot(s_k, [q])[0])
+                rho.append(1 / d(y_k, s_k))
+                alpha.append(rho[-1] * d(s_k, q))
                 q = addProd(q, y_k, -alpha[-1])
             rho.reverse()
             alpha.reverse()
             s_k, y_k = history[-1]
-            c = dot(s_k, [y_k])[0] / dot(y_k, [y_k])[0]
-            if c < 1e-10:
+            c = d(s_k, y_k) / d(y_k, y_k)
+            if dot_dev is not None:
+                c = torch.where(c < 1e-10, torch.ones_like(c), c)
+            elif c < 1e-10:
                 c = 1
             q = prod(q, c)
             for k, (s_k, y_k) in enumerate(history):
-                beta = rho[k] * dot(y_k, [q])[0]
+                beta = rho[k] * d(y_k, q)
                 q = addProd(q, s_k, alpha[k] - beta)
         else:
             history = []

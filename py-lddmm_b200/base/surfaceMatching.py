@@ -190,10 +190,19 @@ class _DeviceMatching:
         _, st = self.objectiveFunDef(control, withTrajectory=True)
         return control, st
 
+    def dotProduct_device(self, g1, g2):
+        """g1.g2 over the controls as an FP64 device scalar (no host synchronisation)."""
+        tot = None
+        for k, v in g1.items():
+            if v is None or g2.get(k) is None:
+                continue
+            t = torch.dot(v.reshape(-1), g2[k].reshape(-1))
+            tot = t if tot is None else tot + t
+        return tot if tot is not None else torch.zeros((), dtype=torch.float64, device=self.x0.device)
+
     def dotProduct_euclidean(self, g1, g2):
-        keys = [k for k in g1 if g1[k] is not None]
-        vals = [sum((g1[k] * gr[k]).sum() for k in keys if gr.get(k) is not None) for gr in g2]
-        return torch.stack([torch.as_tensor(v, dtype=torch.float64, device=self.x0.device) for v in vals]).tolist()
+        vals = [self.dotProduct_device(g1, gr) for gr in g2]
+        return torch.stack(vals).tolist()
 
     dotProduct = dotProduct_euclidean
 
