@@ -207,19 +207,23 @@ def data_term_fixtures(kf, sd, surf, shapes, out):
             out[f'data_L{level}_s{sigma}'] = rec
 
 
-def matching_fixtures(kf, surf, sm_mod, so_mod, shapes, out, iters):
+def matching_fixtures(kf, surf, sm_mod, so_mod, shapes, out, iters, laplacian=False):
     """End-to-end runs of SurfaceMatching / SecondOrderSurfaceMatching (base/surfaceMatching.py:75,
     base/secondOrderSurfaceMatching.py:41) with BFGS (base/bfgs.py:55): objective at iteration 0, the first
-    gradient and the objective after each of `iters` iterations."""
+    gradient and the objective after each of `iters` iterations. With `laplacian`, the deformation kernel is the
+    reference's Laplacian kernel of order 3 (fixtures matching_*_lap_L2)."""
     x0, faces = shapes.icosphere(2)
     x1 = shapes.bumpy_ellipsoid(x0, seed=0)
+    tag = '_lap' if laplacian else ''
     for name, cls in (('first', sm_mod.SurfaceMatching), ('second', so_mod.SecondOrderSurfaceMatching)):
         objs = []
         with tempfile.TemporaryDirectory() as tmp:
             fv0 = surf.Surface(surf=(faces, x0))
             fv1 = surf.Surface(surf=(faces, x1))
             opts = dict(outputDir=tmp, mode='normal', maxIter=iters, affine='none', regWeight=1.0,
-                        KparDiff=kf.Kernel(name='gauss', sigma=0.5), KparDist=('gauss', 0.3), sigmaError=1.0,
+                        KparDiff=(kf.Kernel(name='laplacian', sigma=0.5, order=3) if laplacian
+                                  else kf.Kernel(name='gauss', sigma=0.5)),
+                        KparDist=('gauss', 0.3), sigmaError=1.0,
                         errorType='varifold', pk_dtype='float64', algorithm='bfgs', timeStep=0.1, saveRate=10 ** 6,
                         verb=False)
             f = cls(Template=fv0, Target=fv1, options=opts)
@@ -234,7 +238,7 @@ def matching_fixtures(kf, surf, sm_mod, so_mod, shapes, out, iters):
             f.endOfIteration = eoi
             f.optimizeMatching()
             key = 'at' if name == 'first' else 'a0'
-            out[f'matching_{name}_L2'] = dict(x0=x0, x1=x1, faces=faces, obj0=obj0, grad0=g0[key],
+            out[f'matching_{name}{tag}_L2'] = dict(x0=x0, x1=x1, faces=faces, obj0=obj0, grad0=g0[key],
                                               objs=np.array(objs), control=f.control[key])
 
 
@@ -261,7 +265,8 @@ def main():
     sys.modules['pointset_distances'] = psd
     shapes = load_shapes()
     out = {}
-    only = args.only.split(',') if args.only else ['kernels', 'shooting', 'laplacian', 'data', 'matching']
+    only = args.only.split(',') if args.only else ['kernels', 'shooting', 'laplacian', 'data', 'matching',
+                                                   'matching_lap']
     if 'kernels' in only:
         kernel_fixtures(kf, shapes, out)
     if 'shooting' in only:
@@ -273,6 +278,9 @@ def main():
     if 'matching' in only:
         from base import surfaceMatching as sm_mod, secondOrderSurfaceMatching as so_mod
         matching_fixtures(kf, surf, sm_mod, so_mod, shapes, out, args.iters)
+    if 'matching_lap' in only:
+        from base import surfaceMatching as sm_mod, secondOrderSurfaceMatching as so_mod
+        matching_fixtures(kf, surf, sm_mod, so_mod, shapes, out, args.iters, laplacian=True)
     save(out)
 
 

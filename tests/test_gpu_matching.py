@@ -1,6 +1,7 @@
 """End-to-end parity of the device-resident matching drivers with the reference's own runs
 (tests/golden/matching_*_L2.npz: SurfaceMatching / SecondOrderSurfaceMatching, level-2 icosphere -> bumpy
-ellipsoid, Gaussian sigma 0.5, varifold sigma 0.3, T = 10, BFGS, 5 iterations, float64).
+ellipsoid, Gaussian or Laplacian (order 3) deformation kernel sigma 0.5, varifold sigma 0.3, T = 10, BFGS,
+5 iterations, float64).
 
 FP64 path: objective at iteration 0 and first gradient within 1e-10, objective after every iteration within 1e-7
 (the same BFGS / weak-Wolfe decisions). FP32 compensated path: objective 1e-6, gradient 2e-5, per-iteration
@@ -16,22 +17,27 @@ from conftest import GOLDEN, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _options(dtype, maxIter):
+def _options(dtype, maxIter, family='gauss'):
     from base.kernelFunctions import Kernel
-    return dict(mode='normal', maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=Kernel(name='gauss', sigma=0.5),
+    K = Kernel(name='laplacian', sigma=0.5, order=3) if family == 'laplacian' else Kernel(name='gauss', sigma=0.5)
+    return dict(mode='normal', maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=K,
                 KparDist=('gauss', 0.3), sigmaError=1.0, errorType='varifold', pk_dtype=dtype, algorithm='bfgs',
                 timeStep=0.1, verb=False)
 
 
+@pytest.mark.parametrize('family', ['gauss', 'laplacian'])
 @pytest.mark.parametrize('order', ['first', 'second'])
 @pytest.mark.parametrize('dtype', ['float64', 'float32'])
-def test_matching_vs_reference(order, dtype):
+def test_matching_vs_reference(order, dtype, family):
+    """Gaussian deformation kernel, or the Laplacian kernel of order 3 (fixtures matching_*_lap_L2)."""
     from base.surfaceMatching import SurfaceMatching, SecondOrderSurfaceMatching
     from base.surfaces import Surface
-    d = np.load(os.path.join(GOLDEN, f'matching_{order}_L2.npz'))
+    tag = '_lap' if family == 'laplacian' else ''
+    d = np.load(os.path.join(GOLDEN, f'matching_{order}{tag}_L2.npz'))
     F = d['faces']
     cls = SurfaceMatching if order == 'first' else SecondOrderSurfaceMatching
-    f = cls(Template=Surface(surf=(F, d['x0'])), Target=Surface(surf=(F, d['x1'])), options=_options(dtype, 5))
+    f = cls(Template=Surface(surf=(F, d['x0'])), Target=Surface(surf=(F, d['x1'])),
+            options=_options(dtype, 5, family))
     t_obj, t_grad, t_it = (1e-10, 1e-10, 1e-7) if dtype == 'float64' else (1e-6, 2e-5, 1e-4)
     obj0 = f.objectiveFun()
     assert abs(obj0 - float(d['obj0'])) < t_obj * abs(float(d['obj0']))

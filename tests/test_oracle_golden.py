@@ -21,7 +21,8 @@ DFILES = sorted(glob.glob(os.path.join(GOLDEN, 'data_*.npz')))
 
 def test_fixtures_present():
     assert len(KFILES) == 4 and len(DFILES) == 4
-    for name in ('first_order_L2', 'second_order_L2', 'matching_first_L2', 'matching_second_L2'):
+    for name in ('first_order_L2', 'second_order_L2', 'matching_first_L2', 'matching_second_L2',
+                 'matching_first_lap_L2', 'matching_second_lap_L2', 'laplacian_shooting_L2_o3'):
         assert os.path.exists(os.path.join(GOLDEN, name + '.npz'))
 
 
