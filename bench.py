@@ -185,7 +185,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     import numba
-    threads = os.cpu_count() or 1
+    threads = numba.config.NUMBA_NUM_THREADS       # every host thread numba may use (NUMBA_NUM_THREADS caps it)
     numba.set_num_threads(threads)
     x, a_raw = workload()
     import oracle as O
@@ -413,8 +413,9 @@ def run_b200(args, rank, world, local_rank):
     traffic = ncu_traffic()
     cb_targets = args.cpu_targets
     import numba
-    numba.set_num_threads(os.cpu_count() or 1)
-    cb_val, cb_dt, cb_pairs = cpu_baseline(x, a, cb_targets, os.cpu_count())
+    cb_threads = numba.config.NUMBA_NUM_THREADS
+    numba.set_num_threads(cb_threads)
+    cb_val, cb_dt, cb_pairs = cpu_baseline(x, a, cb_targets, cb_threads)
     line = {
         'metric': METRIC, 'value': value, 'unit': 'pairs/s', 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
@@ -427,7 +428,7 @@ def run_b200(args, rank, world, local_rank):
                      'ops_per_pair': {'fp32': OPS_FP32_PER_PAIR, 'sfu': OPS_SFU_PER_PAIR},
                      'peak_source': f'{n_sm} SMs x 128 FP32 lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
                                     f'max SM clock; MEASURED_PEAKS.json has no FP32 figure)'},
-        'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': os.cpu_count(), 'kind': 'port',
+        'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': cb_threads, 'kind': 'port',
                          'sample': f'{cb_pairs:.3g} pairs: blocks of {cb_targets} targets x {n} sources x '
                                    f'{len(SIGMAS)} widths, float64 numba oracle, {cb_dt:.1f} s'},
         'clocks': clocks, 'gpu_launches': launches,
