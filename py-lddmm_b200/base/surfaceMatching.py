@@ -113,6 +113,7 @@ class _DeviceMatching:
         self.history = []
         self.times = []
         self._last_trial = None
+        self._grad_cache = None
         self._control_version = 0
         self.control = Control()
         self.controlTry = Control()
@@ -168,6 +169,17 @@ class _DeviceMatching:
             self.stateTry = st
             self.objTry = objTry
         return objTry
+
+    def getGradient(self, coeff=1.0, update=None):
+        """The optimiser's gradient at the current control, or at control - update[1] * update[0]. The gradient at
+        the current control is kept until the control, its tensors or the precision change: optimizeMatching asks
+        for it once for the gradient threshold and BFGS again for its first step."""
+        if update is not None:
+            return self._gradient(coeff, update)
+        key = (self._control_version, self._control_key(), float(coeff), str(self.options['KparDiff'].pk_dtype))
+        if self._grad_cache is None or self._grad_cache[0] != key:
+            self._grad_cache = (key, self._gradient(coeff))
+        return self._grad_cache[1]
 
     def acceptVarTry(self):
         self.obj = self.objTry
@@ -268,7 +280,7 @@ class SurfaceMatching(_DeviceMatching):
         st = State(xt=xt)
         return (e[0], st) if withTrajectory or withJacobian else e[0]
 
-    def getGradient(self, coeff=1.0, update=None):
+    def _gradient(self, coeff=1.0, update=None):
         """(base/surfaceMatching.py:1040-1105, euclidean gradient K(x_t)(2 w a_t - p_{t+1}) / (coeff T))."""
         if update is None:
             control, st = self.control, self.state
@@ -312,7 +324,7 @@ class SecondOrderSurfaceMatching(_DeviceMatching):
         st = State(xt=xt, at=at)
         return (obj, st) if withTrajectory or withJacobian else obj
 
-    def getGradient(self, coeff=1.0, update=None):
+    def _gradient(self, coeff=1.0, update=None):
         """da0 = K(x0)a0 - pa_0 after the adjoint sweep (base/secondOrderPointSetMatching.py:379-483)."""
         if update is None:
             control, st = self.control, self.state
