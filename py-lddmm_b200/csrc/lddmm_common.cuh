@@ -20,6 +20,7 @@
 // FP64 path (the faithful baseline): the same pair functors instantiated with double, exp() and FP64 sums.
 #pragma once
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include <type_traits>
@@ -29,6 +30,9 @@
 #endif
 #ifndef LDDMM_COMP_SMEM
 #define LDDMM_COMP_SMEM 1  // 0: keep every op's compensated (hi, lo) sums in registers
+#endif
+#ifndef LDDMM_CULL
+#define LDDMM_CULL 1  // 0: no exact culling of far tile pairs (no box pre-pass)
 #endif
 #ifndef LDDMM_SOURCE_UNROLL
 #define LDDMM_SOURCE_UNROLL 4  // unroll depth of the per-source loop over a shared-memory tile
@@ -204,18 +208,71 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   return y;
 }
 
+// kCullR2<V>: a scaled squared distance beyond which every radial factor is exactly zero in the arithmetic of V
+// (FP32: ex2.approx.ftz of an argument below -126 flushes to +0; FP64: exp below -745.2 underflows to 0), with a
+// margin for the FP32 rounding of the box test that uses it.
 struct Gauss {
   template <typename V>
   static __device__ __forceinline__ KV<V> eval(const Frame&, V r2) {
     const V e = VT<V>::expneg(r2);
     return {e, e, e};
   }
+  template <typename V>
+  static constexpr float kCullR2 = VT<V>::kLanes == 2 ? 127.0f : 746.0f;
 };
 
 struct Laplacian {
   template <typename V>
   static __device__ __forceinline__ KV<V> eval(const Frame& f, V r2);
+  template <typename V>
+  static constexpr float kCullR2 = VT<V>::kLanes == 2 ? 127.0f * 127.0f : 746.0f * 746.0f;  // the radius u = |d|
 };
+
+// Axis-aligned box of the scaled coordinates held by a block of threads: per-thread (lo, hi), reduced over the
+// block through `red` (6 x warps floats). Every thread ends with the block's box; callers separate reuses of `red`
+// by a barrier.
+template <int TPB>
+__device__ __forceinline__ void block_box(float lo[3], float hi[3], float (*red)[TPB / 32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[c] = fminf(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      red[c][warp] = lo[c];
+      red[3 + c][warp] = hi[c];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    lo[c] = red[c][0];
+    hi[c] = red[3 + c][0];
+#pragma unroll
+    for (int w = 1; w < TPB / 32; ++w) {
+      lo[c] = fminf(lo[c], red[c][w]);
+      hi[c] = fmaxf(hi[c], red[3 + c][w]);
+    }
+  }
+}
+
+// Squared distance between two boxes (0 when they overlap).
+__device__ __forceinline__ float box_gap2(const float alo[3], const float ahi[3], const float blo[3],
+                                          const float bhi[3]) {
+  float d2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float g = fmaxf(0.f, fmaxf(blo[c] - ahi[c], alo[c] - bhi[c]));
+    d2 = fmaf(g, g, d2);
+  }
+  return d2;
+}
 
 __device__ __forceinline__ float horner5(const float* c, float u) {
   return fmaf(fmaf(fmaf(fmaf(c[4], u, c[3]), u, c[2]), u, c[1]), u, c[0]);
@@ -270,6 +327,7 @@ __device__ __forceinline__ V tgt_field(const double* __restrict__ p, int stride,
 struct SKPlan {
   int gx = 0, TT = 0, C = 0, S = 0;  // S = max partial slots per target block
   long long W = 0;
+  size_t box_off = 0;   // byte offset of the (gx + TT) coordinate boxes after the partial slots
   size_t ws_bytes = 0;
 };
 
@@ -302,7 +360,8 @@ inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int 
     if (c1 - c0 + 1 > smax) smax = c1 - c0 + 1;
   }
   p.S = smax;
-  p.ws_bytes = (size_t)p.S * (size_t)na * (size_t)n * partial_bytes;
+  p.box_off = ((size_t)p.S * (size_t)na * (size_t)n * partial_bytes + 255) & ~(size_t)255;
+  p.ws_bytes = p.box_off + (size_t)(p.gx + p.TT) * 6 * sizeof(float);
   return p;
 }
 
@@ -316,10 +375,27 @@ inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int 
 //   Op::template pair<V, Fam>(const Frame&, tgt, const V* s, V* acc)   (Fam: Gauss or Laplacian)
 // Output: ws[(slot * NA + c) * n + i] = compensated partial of accumulator c of target i for one segment.
 // ---------------------------------------------------------------------------------------------------------
+// Ops may ask for a minimum number of resident CTAs per SM (`static constexpr int kMinCtas`), which caps the
+// registers the compiler may use (65536 / (TPB * kMinCtas)).
+// The cap applies to the FP32 (F2) kernels only.
+template <class Op, typename V, class = void>
+struct MinCtas : std::integral_constant<int, LDDMM_MIN_CTAS> {};
+template <class Op>
+struct MinCtas<Op, F2, std::void_t<decltype(Op::kMinCtas)>> : std::integral_constant<int, Op::kMinCtas> {};
+
+// Ops whose sums are culled declare `static constexpr bool kCull = true;`: the surface data terms, whose faces are
+// stored in a spatially coherent order by mesh generators and whose widths are often small against the shape.
+// Elsewhere the box pre-pass and the per-tile test cost 2-3% and seldom pay (vertex orders are less coherent, and
+// deformation widths large), so the other ops evaluate every tile.
+template <class Op, class = void>
+struct Culled : std::false_type {};
+template <class Op>
+struct Culled<Op, std::void_t<decltype(Op::kCull)>> : std::bool_constant<LDDMM_CULL != 0 && Op::kCull> {};
+
 template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
-__global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
+__global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
     pairs_kernel(const typename Op::Params P, int n, int m, int TT, long long W, int C,
-                 typename VT<V>::Partial* __restrict__ ws) {
+                 typename VT<V>::Partial* __restrict__ ws, const float* __restrict__ boxes) {
   constexpr int L = VT<V>::kLanes;
   constexpr int G = RT / L;  // lane groups per thread
   constexpr int NU = (Op::NS + 1) / 2;
@@ -329,6 +405,12 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
   // the op keeps them in registers; shared memory frees 2-4 registers per accumulator for more resident warps.
   constexpr bool kSm = LDDMM_COMP_SMEM && !CompInRegisters<Op>::value;
   __shared__ V cs[kSm ? G * Op::NA * Comp<V>::kWords : 1][TPB];
+  // Exact culling (ops with Culled<Op>): a (target block, source tile) unit whose coordinate boxes (box_kernel) are
+  // farther apart than the distance at which the kernel's radial factors are exactly zero in this arithmetic
+  // contributes exactly nothing, and is skipped by the whole CTA.
+  constexpr float kZeroR2 = Fam::template kCullR2<V>;
+  const int gx = (n + TPB * RT - 1) / (TPB * RT);
+  __shared__ float tbox[6];  // the segment's target box, in shared memory (re-read per tile, not held in registers)
 
   const long long u_end = sk_start(blockIdx.x + 1, W, C);
   long long u = sk_start(blockIdx.x, W, C);
@@ -354,8 +436,17 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
         if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
       }
     }
+    if constexpr (Culled<Op>::value) {
+      __syncthreads();  // the previous segment's last tile test has read tbox
+      if (threadIdx.x < 6) tbox[threadIdx.x] = boxes[6 * tb + threadIdx.x];
+      __syncthreads();
+    }
 
     for (int j = j0; j < j1; ++j) {
+      if constexpr (Culled<Op>::value) {
+        const float* sbox = boxes + 6 * (gx + j);
+        if (box_gap2(tbox, tbox + 3, sbox, sbox + 3) > kZeroR2) continue;  // uniform over the CTA
+      }
       const int l = j * TPB + threadIdx.x;
       {
         double f[2 * NU];
@@ -416,6 +507,55 @@ __global__ void __launch_bounds__(TPB, LDDMM_MIN_CTAS)
   }
 }
 
+// Coordinate boxes for exact culling, from the same scaled coordinates the pair kernel uses: block b < gx covers
+// target block b (its TPB * RT targets), block gx + j source tile j. boxes[6 b ..] = (lo xyz, hi xyz).
+template <class Op, typename V, int TPB, int RT>
+__global__ void __launch_bounds__(TPB) box_kernel(const typename Op::Params P, int n, int m, int gx,
+                                                  float* __restrict__ boxes) {
+  constexpr int L = VT<V>::kLanes;
+  constexpr int G = RT / L;
+  constexpr int NU = (Op::NS + 1) / 2;
+  __shared__ float red[6][TPB / 32];
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  const int b = blockIdx.x;
+  if (b < gx) {
+    const int base = b * (TPB * RT) + threadIdx.x;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      int i0 = base + (g * L) * TPB, i1 = base + (g * L + L - 1) * TPB;
+      i0 = i0 < n ? i0 : n - 1;
+      i1 = i1 < n ? i1 : n - 1;
+      typename Op::template Tgt<V> t;
+      Op::template load_target<V>(P, i0, i1, t);
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const float y[3] = {(float)VT<V>::lane(t.y0, k), (float)VT<V>::lane(t.y1, k), (float)VT<V>::lane(t.y2, k)};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          lo[c] = fminf(lo[c], y[c]);
+          hi[c] = fmaxf(hi[c], y[c]);
+        }
+      }
+    }
+  } else {
+    const int l = (b - gx) * TPB + threadIdx.x;
+    if (l < m) {
+      double f[2 * NU];
+      Op::source_fields(P, l, f);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) lo[c] = hi[c] = (float)f[c];
+    }
+  }
+  block_box<TPB>(lo, hi, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      boxes[6 * b + c] = lo[c];
+      boxes[6 * b + 3 + c] = hi[c];
+    }
+  }
+}
+
 // Epilogue: reduce the partial slots of target i (its block's CTAs, in CTA order) in FP64, then Op::finalize.
 template <class Op, typename V>
 __global__ void finalize_kernel(const typename Op::Params P, int n, int tb_targets, int TT, long long W, int C,
@@ -460,9 +600,13 @@ inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* w
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (plan.ws_bytes > 0 && ws == nullptr) return kInvalidArgument;
   auto* part = reinterpret_cast<typename VT<V>::Partial*>(ws);
-  if (plan.W > 0)
+  if (plan.W > 0) {
+    float* boxes = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.box_off);
+    if (Culled<Op>::value)
+      box_kernel<Op, V, TPB, RT><<<plan.gx + plan.TT, TPB, 0, stream>>>(P, (int)n, (int)m, plan.gx, boxes);
     pairs_kernel<Op, V, TPB, RT, Fam><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C,
-                                                                   part);
+                                                                   part, boxes);
+  }
   const int fb = 256;
   finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, TPB * RT, plan.TT, plan.W, plan.C,
                                                                       part);

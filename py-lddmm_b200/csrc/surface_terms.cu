@@ -98,6 +98,7 @@ __device__ __forceinline__ void load_face_target(const FaceRec* T, const Frame& 
 template <int KIND>
 struct OpSurfEnergy {
   static constexpr int NS = 7, NA = (KIND == LDDMM_DATA_CURRENT) ? 3 : 1;
+  static constexpr bool kCull = true;  // exact culling of far face tiles
   static constexpr bool kCompInRegisters = true;  // measured faster than shared memory for this op
   struct Params {
     const FaceRec* T;
@@ -148,6 +149,7 @@ struct FaceGrad {
 template <int KIND>
 struct OpSurfGrad {
   static constexpr int NS = 7, NA = (KIND == LDDMM_DATA_VARIFOLD) ? 8 : (KIND == LDDMM_DATA_CURRENT ? 6 : 4);
+  static constexpr bool kCull = true;  // exact culling of far face tiles
   struct Params {
     const FaceRec* T;
     FaceSources S;
