@@ -12,7 +12,7 @@ reference itself (tests/golden/make_golden.py, tests/test_oracle_golden.py).
 from .kernels import (apply_k, apply_diff_kt, apply_ddiff_k11and12, apply_diff_k1and2, apply_divergence,
                       apply_k_tensor, apply_k_mat, apply_diff_k_mat)
 from . import laplacian
-from .shooting import (landmark_direct_evolution_euler, landmark_hamiltonian_gradient,
+from .shooting import (landmark_direct_evolution_euler, landmark_hamiltonian_gradient, landmark_epdiff,
                        second_order_evolution, second_order_gradient)
 from .surface_terms import (face_geometry, varifold_norm0, varifold_norm_def, varifold_norm_gradient,
                             current_norm0, current_norm_def, current_norm_gradient,

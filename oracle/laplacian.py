@@ -172,4 +172,5 @@ def ops(order):
         apply_k=lambda y, x, a, s: apply_k(y, x, a, s, order),
         apply_diff_kt=lambda y, x, p, a, s, **kw: apply_diff_kt(y, x, p, a, s, order=order, **kw),
         apply_ddiff_k11and12=lambda x, n, a, p, s: apply_ddiff_k11and12(x, n, a, p, s, order),
-        apply_diff_k1and2=lambda x, a1, a2, s: apply_diff_k1and2(x, a1, a2, s, order))
+        apply_diff_k1and2=lambda x, a1, a2, s: apply_diff_k1and2(x, a1, a2, s, order),
+        apply_divergence=lambda y, x, a, s: apply_divergence(y, x, a, s, order))

@@ -11,7 +11,8 @@ from . import kernels as _gauss
 
 GAUSS = types.SimpleNamespace(apply_k=_gauss.apply_k, apply_diff_kt=_gauss.apply_diff_kt,
                               apply_ddiff_k11and12=_gauss.apply_ddiff_k11and12,
-                              apply_diff_k1and2=_gauss.apply_diff_k1and2)
+                              apply_diff_k1and2=_gauss.apply_diff_k1and2,
+                              apply_divergence=_gauss.apply_divergence)
 
 
 def landmark_direct_evolution_euler(x0, at, sigma, ops=GAUSS):
@@ -54,6 +55,40 @@ def second_order_evolution(x0, a0, sigma, timeStep, ops=GAUSS):
         xt[k + 1] = x + timeStep * zx
         at[k + 1] = a + timeStep * za
     return xt, at
+
+
+def landmark_epdiff(T, x0, a0, sigma, point_set=None, normals=None, jacobian=False, ops=GAUSS):
+    """landmarkEPDiff (base/pointEvolution.py:320-382): T steps of 1/T of x += dt K(x) a, a -= dt DK^T(x; a, a)
+    (momentum kept for steps 0..T-1), with a point set carried by y += dt K(x, y) a, normals by
+    n -= dt DK^T(x; n, a) and the log-Jacobian by J += dt div(K a)(x). Returns the reference's list
+    [xt, at, (yt), (nt), (Jt)], or (xt, at) with nothing extra requested."""
+    T = int(T)
+    dt = 1.0 / T
+    xt = np.zeros((T + 1,) + x0.shape)
+    at = np.zeros((T,) + x0.shape)
+    xt[0], at[0] = x0, a0
+    out_y = out_n = out_j = None
+    if point_set is not None:
+        out_y = np.zeros((T + 1,) + point_set.shape)
+        out_y[0] = point_set
+    if normals is not None:
+        out_n = np.zeros((T + 1,) + normals.shape)
+        out_n[0] = normals
+    if jacobian:
+        out_j = np.zeros((T + 1, x0.shape[0], 1))
+    for k in range(T):
+        x, a = xt[k], at[k]
+        xt[k + 1] = x + dt * ops.apply_k(x, x, a, sigma)
+        if k < T - 1:
+            at[k + 1] = a - dt * ops.apply_diff_kt(x, x, a, a, sigma)
+        if out_y is not None:
+            out_y[k + 1] = out_y[k] + dt * ops.apply_k(out_y[k], x, a, sigma)
+        if out_n is not None:
+            out_n[k + 1] = out_n[k] - dt * ops.apply_diff_kt(x, x, out_n[k], a, sigma)
+        if out_j is not None:
+            out_j[k + 1] = out_j[k] + dt * ops.apply_divergence(x, x, a, sigma).reshape(-1, 1)
+    extra = [v for v in (out_y, out_n, out_j) if v is not None]
+    return (xt, at) if not extra else [xt, at] + extra
 
 
 def second_order_gradient(x0, a0, px1, pa1, sigma, timeStep, ops=GAUSS):

@@ -217,6 +217,41 @@ def secondOrderEvolution(x0, a0, KparDiff, timeStep, withSpline=None, affine=Non
     return {'xt': _ret(xt, like_np), 'at': _ret(at, like_np), 'Jt': _ret(Jt, like_np), 'yt': _ret(zt, like_np)}
 
 
+def landmarkEPDiff(T, x0, a0, KparDiff, affine=None, withJacobian=False, withNormals=None, withPointSet=None):
+    """Geodesic (EPDiff) shooting over T steps of 1/T (base/pointEvolution.py:320-382): xt (T+1,N,3) and at (T,N,3)
+    from the fused shooting kernels; with a point set, normals or the Jacobian requested, the list
+    [xt, at, (yt), (nt), (Jt)] in the reference's order (yt carried by K(x_t, .) a_t, nt by -DK^T(x_t; n_t, a_t),
+    Jt by the divergence of K(x_t, .) a_t at the points x_t)."""
+    _no_affine(affine)
+    like_np = _is_np(x0)
+    X0, A0 = nat.as_device(x0), nat.as_device(a0)
+    T = int(T)
+    dt = 1.0 / T
+    xt, at_all = shoot_second_order(X0, A0, KparDiff, dt)
+    at = at_all[:T]
+    out = [_ret(xt, like_np), _ret(at.contiguous(), like_np)]
+    if withPointSet is not None:
+        Y0 = nat.as_device(withPointSet)
+        yt = torch.empty((T + 1,) + tuple(Y0.shape), dtype=torch.float64, device=X0.device)
+        yt[0] = Y0
+        for k in range(T):
+            yt[k + 1] = yt[k] + dt * KparDiff.applyK(xt[k], at[k], firstVar=yt[k])
+        out.append(_ret(yt, like_np))
+    if withNormals is not None:
+        N0 = nat.as_device(withNormals)
+        nt = torch.empty((T + 1,) + tuple(N0.shape), dtype=torch.float64, device=X0.device)
+        nt[0] = N0
+        for k in range(T):
+            nt[k + 1] = nt[k] - dt * KparDiff.applyDiffKT(xt[k], nt[k], at[k])
+        out.append(_ret(nt, like_np))
+    if withJacobian:
+        Jt = torch.zeros((T + 1, X0.shape[0], 1), dtype=torch.float64, device=X0.device)
+        for k in range(T):
+            Jt[k + 1] = Jt[k] + dt * KparDiff.applyDivergence(xt[k], at[k])
+        out.append(_ret(Jt, like_np))
+    return (out[0], out[1]) if len(out) == 2 else out
+
+
 def secondOrderHamiltonian(x, a, px, pa, KparDiff, withSpline=None, affine=None):
     """H = px.K(x)a - pa.DK^T(x; a, a) (base/pointEvolution.py:475-486)."""
     _no_affine(affine)

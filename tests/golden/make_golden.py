@@ -137,6 +137,19 @@ def shooting_fixtures(kf, evol, shapes, out):
                                   xt=fw['xt'], at=fw['at'], da0=g['da0'], pxt=g['pxt'], pat=g['pat'])
 
 
+def epdiff_fixtures(kf, evol, shapes, out):
+    """landmarkEPDiff (base/pointEvolution.py:320-382) with a point set and normals. (withJacobian=True raises in
+    the reference: line 366 adds an (N,1) divergence to an (N,) slice.)"""
+    rng = np.random.default_rng(77)
+    x0, _ = shapes.icosphere(2)
+    K = kf.Kernel(name='gauss', sigma=0.5)
+    a0 = smooth_momenta(kf, shapes, x0, rng, 0.4, vmax=0.3)
+    y0 = shapes.bumpy_ellipsoid(x0, seed=3)[:40] * 0.9
+    n0 = rng.normal(size=x0.shape)
+    xt, at, yt, nt = evol.landmarkEPDiff(8, x0, a0, K, withNormals=n0, withPointSet=y0)
+    out['epdiff_L2'] = dict(x0=x0, a0=a0, y0=y0, n0=n0, sigma=0.5, T=8, xt=xt, at=at, yt=yt, nt=nt)
+
+
 def laplacian_fixtures(kf, evol, shapes, out):
     """The same operators and both shooting variants with the reference's Laplacian kernel
     (KernelSpec(name='laplacian', order=q), base/kernelFunctions.py:363-368; lap_fun* at
@@ -265,12 +278,14 @@ def main():
     sys.modules['pointset_distances'] = psd
     shapes = load_shapes()
     out = {}
-    only = args.only.split(',') if args.only else ['kernels', 'shooting', 'laplacian', 'data', 'matching',
-                                                   'matching_lap']
+    only = args.only.split(',') if args.only else ['kernels', 'shooting', 'epdiff', 'laplacian', 'data',
+                                                   'matching', 'matching_lap']
     if 'kernels' in only:
         kernel_fixtures(kf, shapes, out)
     if 'shooting' in only:
         shooting_fixtures(kf, evol, shapes, out)
+    if 'epdiff' in only:
+        epdiff_fixtures(kf, evol, shapes, out)
     if 'laplacian' in only:
         laplacian_fixtures(kf, evol, shapes, out)
     if 'data' in only:

@@ -45,6 +45,26 @@ def test_second_order_vs_reference(dtype):
     assert rel_err(fw['xt'], d['xt']) < TOL[dtype]
 
 
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+def test_landmark_epdiff_vs_reference(dtype):
+    """landmarkEPDiff with a point set and normals against the reference's output; the Jacobian (which the
+    reference's line cannot return: it broadcasts an (N,1) divergence into an (N,) slice) against the oracle."""
+    import oracle as O
+    from base import pointEvolution as evol
+    d = np.load(os.path.join(GOLDEN, 'epdiff_L2.npz'))
+    K = kernel(float(d['sigma']), dtype)
+    T = int(d['T'])
+    xt, at, yt, nt = evol.landmarkEPDiff(T, d['x0'], d['a0'], K, withNormals=d['n0'], withPointSet=d['y0'])
+    for k, v in (('xt', xt), ('at', at), ('yt', yt), ('nt', nt)):
+        assert v.shape == d[k].shape, k
+        assert rel_err(v, d[k]) < TOL[dtype], (k, rel_err(v, d[k]))
+    xs, as_ = evol.landmarkEPDiff(T, d['x0'], d['a0'], K)
+    assert rel_err(xs, d['xt']) < TOL[dtype] and rel_err(as_, d['at']) < TOL[dtype]
+    _, _, Jt = evol.landmarkEPDiff(T, d['x0'], d['a0'], K, withJacobian=True)
+    _, _, Jref = O.landmark_epdiff(T, d['x0'], d['a0'], float(d['sigma']), jacobian=True)
+    assert Jt.shape == Jref.shape and rel_err(Jt, Jref) < TOL[dtype]
+
+
 def test_second_order_l4_vs_oracle():
     import oracle as O
     from base import pointEvolution as evol

@@ -22,7 +22,7 @@ DFILES = sorted(glob.glob(os.path.join(GOLDEN, 'data_*.npz')))
 def test_fixtures_present():
     assert len(KFILES) == 4 and len(DFILES) == 4
     for name in ('first_order_L2', 'second_order_L2', 'matching_first_L2', 'matching_second_L2',
-                 'matching_first_lap_L2', 'matching_second_lap_L2', 'laplacian_shooting_L2_o3'):
+                 'matching_first_lap_L2', 'matching_second_lap_L2', 'laplacian_shooting_L2_o3', 'epdiff_L2'):
         assert os.path.exists(os.path.join(GOLDEN, name + '.npz'))
 
 
@@ -65,6 +65,14 @@ def test_second_order_shooting():
     g = O.second_order_gradient(d['x0'], d['a0'], d['px1'], d['pa1'], float(d['sigma']), float(d['timeStep']))
     for k in ('xt', 'at', 'da0', 'pxt', 'pat'):
         assert rel_err(g[k], d[k]) < 1e-12, k
+
+
+def test_landmark_epdiff():
+    d = np.load(os.path.join(GOLDEN, 'epdiff_L2.npz'))
+    xt, at, yt, nt = O.landmark_epdiff(int(d['T']), d['x0'], d['a0'], float(d['sigma']), point_set=d['y0'],
+                                       normals=d['n0'])
+    for k, v in (('xt', xt), ('at', at), ('yt', yt), ('nt', nt)):
+        assert rel_err(v, d[k]) < 1e-12, k
 
 
 @pytest.mark.parametrize('path', DFILES, ids=os.path.basename)
