@@ -9,9 +9,10 @@ compensated accumulation and FP64 outputs.
             by writing a 256 MiB buffer; the flush is outside the timed events)
   e2e       the same step through the reference-facing API `Kernel.applyK(x, a)` with numpy (host) arrays:
             host->device copy of x and a, the kernels, device->host copy of the result, every step
-  roofline  the pair kernel against the FP32 pipe: 9 FP32 lane-ops + 1 SFU op per pair (3 differences,
-            3 FMAs for the scaled squared distance, 3 FMAs accumulating K a, one ex2);
-            peak = 148 SMs x 128 FP32 lanes x max SM clock
+  roofline  the pair kernel against the MUFU (ex2) pipe, its binding pipe: 1 SFU op + 6 FP32 lane-ops per pair
+            (expanded-distance form: 3 FMAs for |x|^2 - 2 y.x about the target block's centre, one ex2, 3 FMAs
+            accumulating K a); peak = 148 SMs x 16 MUFU lanes x max SM clock (the FP32 fraction is reported
+            beside it against 148 x 128 FP32 lanes x max SM clock)
   cpu_baseline  the CPU oracle (numba, float64, all host threads) on a bounded sample of the same sums
 
 `--impl reference` times the CPU implementation of the same sums (the oracle restatement of the reference's
@@ -42,7 +43,7 @@ sys.path.insert(0, REPO)
 
 LEVEL = 6
 SIGMAS = (0.25, 0.5)
-OPS_FP32_PER_PAIR = 9
+OPS_FP32_PER_PAIR = 6
 OPS_SFU_PER_PAIR = 1
 METRIC = 'Gauss kernel pairs/s'
 
@@ -407,9 +408,10 @@ def run_b200(args, rank, world, local_rank):
     sm_max = clocks.get('sm_max_mhz') or peaks.get('sm_max_mhz') or 1965.0
     n_sm = torch.cuda.get_device_properties(0).multi_processor_count
     peak_fp32 = n_sm * 128 * sm_max * 1e6 / 1e12          # T lane-ops/s
+    peak_sfu = n_sm * 16 * sm_max * 1e6 / 1e12            # T ex2/s
     mean_launch_s = statistics.mean(launch_ms) * 1e-3
-    achieved = n * n * OPS_FP32_PER_PAIR / mean_launch_s / 1e12
-    sfu_frac = (n * n * OPS_SFU_PER_PAIR / mean_launch_s) / (n_sm * 16 * sm_max * 1e6)
+    achieved = n * n * OPS_SFU_PER_PAIR / mean_launch_s / 1e12
+    fp32_frac = (n * n * OPS_FP32_PER_PAIR / mean_launch_s / 1e12) / peak_fp32
     traffic = ncu_traffic()
     cb_targets = args.cpu_targets
     import numba
@@ -422,12 +424,12 @@ def run_b200(args, rank, world, local_rank):
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': config(n),
         'e2e': {'value': e2e_value, 'unit': 'pairs/s', 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
                 'ms_per_step': float(te) / args.steps, 'api': 'Kernel.applyK(numpy x, numpy a)'},
-        'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak_fp32, 'unit': 'T FP32 lane-ops/s',
-                     'frac': achieved / peak_fp32, 'sfu_frac': sfu_frac, 'traffic': traffic,
-                     'kernel': 'pairs_kernel<OpK, F2, 128, 4, Gauss> + finalize_kernel (timed together per call)',
+        'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak_sfu, 'unit': 'T ex2/s',
+                     'frac': achieved / peak_sfu, 'fp32_frac': fp32_frac, 'traffic': traffic,
+                     'kernel': 'pairs_kernel_x<OpK, 128, 8> + finalize_kernel (timed together per call)',
                      'ops_per_pair': {'fp32': OPS_FP32_PER_PAIR, 'sfu': OPS_SFU_PER_PAIR},
-                     'peak_source': f'{n_sm} SMs x 128 FP32 lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
-                                    f'max SM clock; MEASURED_PEAKS.json has no FP32 figure)'},
+                     'peak_source': f'{n_sm} SMs x 16 MUFU lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
+                                    f'max SM clock; MEASURED_PEAKS.json has no MUFU or FP32 figure)'},
         'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': cb_threads, 'kind': 'port',
                          'sample': f'{cb_pairs:.3g} pairs: blocks of {cb_targets} targets x {n} sources x '
                                    f'{len(SIGMAS)} widths, float64 numba oracle, {cb_dt:.1f} s'},

@@ -99,8 +99,11 @@ class Kernel(KernelSpec):
 
     def _multi(self, fn):
         """sum_s w_s fn(sigma_s); one launch per width."""
+        scales = self._scales()
+        if len(scales) == 1 and scales[0][1] == 1.0:
+            return fn(scales[0][0])        # one width: no weighting pass
         res = None
-        for s, w in self._scales():
+        for s, w in scales:
             r = fn(s)
             res = r * w if res is None else res + r * w
         return res

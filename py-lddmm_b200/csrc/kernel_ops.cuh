@@ -53,6 +53,25 @@ struct OpK {
     acc[1] = fma(k.k0, s[4], acc[1]);
     acc[2] = fma(k.k0, s[5], acc[2]);
   }
+  // expanded-distance Gaussian form (pairs_kernel_x): payload a, K a accumulated from the kernel value e
+  static constexpr bool kExpand = true;
+  static constexpr int NP = 3;
+  template <typename V> struct TgtX {};
+  template <typename V>
+  static __device__ __forceinline__ void load_target_x(const Params&, int, int, TgtX<V>&) {}
+  static __device__ __forceinline__ void target_point(const Params& P, int i, double* c) {
+    c[0] = P.y[3 * i]; c[1] = P.y[3 * i + 1]; c[2] = P.y[3 * i + 2];
+  }
+  static __device__ __forceinline__ void source_point(const Params& P, int l, double* c, double* f) {
+    c[0] = P.x[3 * l]; c[1] = P.x[3 * l + 1]; c[2] = P.x[3 * l + 2];
+    f[0] = P.a[3 * l]; f[1] = P.a[3 * l + 1]; f[2] = P.a[3 * l + 2];
+  }
+  template <typename V>
+  static __device__ __forceinline__ void accumulate(const TgtX<V>&, V e, const V* s, V* acc) {
+    acc[0] = fma(e, s[0], acc[0]);
+    acc[1] = fma(e, s[1], acc[1]);
+    acc[2] = fma(e, s[2], acc[2]);
+  }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     if (P.dots)
       P.dots[i] = P.dotw[3 * i] * acc[0] + P.dotw[3 * i + 1] * acc[1] + P.dotw[3 * i + 2] * acc[2];

@@ -28,11 +28,24 @@
 #ifndef LDDMM_MIN_CTAS
 #define LDDMM_MIN_CTAS 1  // minimum resident CTAs per SM requested from ptxas (caps registers when > 1)
 #endif
+// per-op minimum resident CTAs (1: no register cap beyond the op's needs)
+#ifndef LDDMM_SOBWD_MIN_CTAS
+#define LDDMM_SOBWD_MIN_CTAS 4  // 124 registers, 4 CTAs per SM: 1.8% faster than 132 and 3 (A/B at level 6)
+#endif
+#ifndef LDDMM_FOBWD_MIN_CTAS
+#define LDDMM_FOBWD_MIN_CTAS 1
+#endif
+#ifndef LDDMM_SURFGRAD_MIN_CTAS
+#define LDDMM_SURFGRAD_MIN_CTAS 1
+#endif
 #ifndef LDDMM_COMP_SMEM
 #define LDDMM_COMP_SMEM 1  // 0: keep every op's compensated (hi, lo) sums in registers
 #endif
 #ifndef LDDMM_CULL
 #define LDDMM_CULL 1  // 0: no exact culling of far tile pairs (no box pre-pass)
+#endif
+#ifndef LDDMM_EXPAND
+#define LDDMM_EXPAND 1  // 0: the Gaussian sums of ops with an expanded-distance form use the difference form
 #endif
 #ifndef LDDMM_SOURCE_UNROLL
 #define LDDMM_SOURCE_UNROLL 4  // unroll depth of the per-source loop over a shared-memory tile
@@ -392,6 +405,32 @@ struct Culled : std::false_type {};
 template <class Op>
 struct Culled<Op, std::void_t<decltype(Op::kCull)>> : std::bool_constant<LDDMM_CULL != 0 && Op::kCull> {};
 
+// Ops with an expanded-distance form of their Gaussian FP32 sums (pairs_kernel_x) declare
+// `static constexpr bool kExpand = true;` and provide
+//   NP                                   payload fields per source (staged after the coordinates)
+//   target_point(P, i, double* c)        raw (unscaled) coordinates of target i
+//   source_point(P, l, double* c, double* pay)   raw coordinates and the NP payload fields of source l
+//   template TgtX<V>, load_target_x<V>(P, i0, i1, TgtX&)   per-lane-group target state besides the coordinates
+//   accumulate<V>(const TgtX&, V e, const V* pay, V* acc)  the pair's contribution from its kernel value e
+template <class Op, class = void>
+struct Expanded : std::false_type {};
+template <class Op>
+struct Expanded<Op, std::void_t<decltype(Op::kExpand)>> : std::bool_constant<LDDMM_EXPAND != 0 && Op::kExpand> {};
+template <class Op, typename V, class Fam>
+constexpr bool kUseExpanded = Expanded<Op>::value && std::is_same<V, F2>::value && std::is_same<Fam, Gauss>::value;
+// pairs_kernel_x's launch shape: 8 targets per thread (4 packed lane groups per source read) with the compensated
+// sums in shared memory (136 registers, 3 CTAs per SM) measured 3-6% faster than the light ops' 4 targets per thread
+// with sums in registers (applyK at levels 6 and 7, varifold energy at level 6)
+#ifndef LDDMM_RT_X
+#define LDDMM_RT_X 8  // targets per thread of pairs_kernel_x (0: the caller's launch shape)
+#endif
+#ifndef LDDMM_X_COMP_SMEM
+#define LDDMM_X_COMP_SMEM 1  // 0: pairs_kernel_x keeps its compensated sums in registers
+#endif
+// Targets per thread of the kernel that runs an op (the plan, the launch and the epilogue all use it).
+template <class Op, typename V, int RT, class Fam>
+constexpr int kRunRT = (kUseExpanded<Op, V, Fam> && LDDMM_RT_X > 0) ? LDDMM_RT_X : RT;
+
 template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 __global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
     pairs_kernel(const typename Op::Params P, int n, int m, int TT, long long W, int C,
@@ -507,6 +546,212 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
   }
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// Expanded-distance Gaussian pair kernel (FP32; ops with Expanded<Op>).
+//
+// With the coordinates of a segment taken relative to the centre o of its target block (the midpoint of the
+// block's coordinate box, scaled units),
+//     2^-|y - x|^2 = 2^-|y|^2 * 2^-(|x|^2 - 2 y.x),
+// and the bracket costs three packed FMAs per pair from the staged fields X = -2 x and q = |x|^2 (the difference
+// form costs three subtractions, a multiply and two FMAs): 6 FP32 lane-ops and one ex2 per pair for K a instead
+// of 9, which leaves the pair loop bound by the MUFU (ex2) pipe instead of the FP32 pipe. The factor 2^-|y|^2 is
+// common to every term of a target and multiplies the segment's compensated sums once, in FP64, when they are
+// written. The identity is exact for the FP32-rounded relative coordinates; the rounding of the bracket grows with
+// |y|^2 and |x|^2 (far sources have a large |x|^2 but terms that are smaller still), so a block is evaluated in the
+// expanded form only when its radius^2 (scaled) is at most kExpandR2, which keeps the relative L2 error of the
+// sums near 1e-6 (FP32 emulation with targets in a ball of that radius: 7e-7 at 32, 1.2e-6 at 64; the difference
+// form: 5e-8); other blocks (point sets in no spatial order, widths small against a block) use the difference form,
+// which costs ~20% more per pair (and, stream-K balancing units rather than time, the kernel waits for the CTAs that
+// drew such blocks). Both forms share the launch plan and the epilogue of pairs_kernel.
+// ---------------------------------------------------------------------------------------------------------
+constexpr float kExpandR2 = 64.0f;
+
+template <class Op, int TPB, int RT>
+__global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
+    pairs_kernel_x(const typename Op::Params P, int n, int m, int TT, long long W, int C,
+                   float2* __restrict__ ws, const float* __restrict__ boxes) {
+  constexpr int L = 2;
+  constexpr int G = RT / L;
+  constexpr int NF = 4 + Op::NP;  // staged fields: X or x (3), q (1), payload (NP)
+  constexpr int NU = (NF + 1) / 2;
+  static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
+  __shared__ Unit<F2> sm[NU][TPB];
+  __shared__ float red[6][TPB / 32];
+  constexpr bool kSm = LDDMM_X_COMP_SMEM != 0;
+  __shared__ F2 cs[kSm ? G * Op::NA * 2 : 1][TPB];
+  const Frame& f = P.f;
+  const double fo[3] = {f.o0, f.o1, f.o2};
+  const int gx = (n + TPB * RT - 1) / (TPB * RT);
+
+  const long long u_end = sk_start(blockIdx.x + 1, W, C);
+  long long u = sk_start(blockIdx.x, W, C);
+  while (u < u_end) {
+    const int tb = (int)(u / TT);
+    const int j0 = (int)(u - (long long)tb * TT);
+    const int j1 = (int)((u_end - (long long)tb * TT) < TT ? (u_end - (long long)tb * TT) : TT);
+    const int slot = (int)blockIdx.x - sk_cta_of((long long)tb * TT, W, C);
+    const int base = tb * (TPB * RT) + threadIdx.x;
+
+    // the block's box and centre (every CTA working on block tb derives the same ones)
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+    for (int t = 0; t < RT; ++t) {
+      int i = base + t * TPB;
+      i = i < n ? i : n - 1;
+      double y[3];
+      Op::target_point(P, i, y);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float v = (float)((y[c] - fo[c]) * f.s);
+        lo[c] = fminf(lo[c], v);
+        hi[c] = fmaxf(hi[c], v);
+      }
+    }
+    block_box<TPB>(lo, hi, red);  // its barrier also orders the previous segment's last tile reads
+    float ob[3], rb2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ob[c] = 0.5f * (lo[c] + hi[c]);
+      const float h = 0.5f * (hi[c] - lo[c]);
+      rb2 = fmaf(h, h, rb2);
+    }
+    const bool expand = rb2 <= kExpandR2;  // uniform over the CTA
+
+    F2 yt[G][3];  // relative scaled target coordinates, lanes = targets (g L, g L + 1) of the thread
+    typename Op::template TgtX<F2> tx[G];
+    Comp<F2> cmp[G][Op::NA];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      int i0 = base + (g * L) * TPB, i1 = base + (g * L + 1) * TPB;
+      i0 = i0 < n ? i0 : n - 1;
+      i1 = i1 < n ? i1 : n - 1;
+      double y0[3], y1[3];
+      Op::target_point(P, i0, y0);
+      Op::target_point(P, i1, y1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        yt[g][c] = f2((float)((y0[c] - fo[c]) * f.s - (double)ob[c]), (float)((y1[c] - fo[c]) * f.s - (double)ob[c]));
+      Op::template load_target_x<F2>(P, i0, i1, tx[g]);
+#pragma unroll
+      for (int c = 0; c < Op::NA; ++c) {
+        cmp[g][c].zero();
+        if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
+      }
+    }
+
+    for (int j = j0; j < j1; ++j) {
+      if constexpr (Culled<Op>::value) {
+        // the same test as pairs_kernel: every term of the unit is exactly zero in the difference form; in the
+        // expanded form each would be below 2^-127 of its payload
+        const float* sbox = boxes + 6 * (gx + j);
+        if (box_gap2(lo, hi, sbox, sbox + 3) > Gauss::kCullR2<F2>) continue;  // uniform over the CTA
+      }
+      const int l = j * TPB + threadIdx.x;
+      {
+        double fl[2 * NU];
+#pragma unroll
+        for (int q = 0; q < 2 * NU; ++q) fl[q] = 0.0;
+        if (l < m) {
+          double xr[3], r2 = 0.0;
+          Op::source_point(P, l, xr, fl + 4);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float xc = (float)((xr[c] - fo[c]) * f.s - (double)ob[c]);
+            r2 += (double)xc * (double)xc;
+            fl[c] = expand ? -2.0 * (double)xc : (double)xc;
+          }
+          fl[3] = r2;
+        }
+#pragma unroll
+        for (int q = 0; q < NU; ++q) {
+          Unit<F2> w;
+          w.a = VT<F2>::dup(fl[2 * q]);
+          w.b = VT<F2>::dup(fl[2 * q + 1]);
+          sm[q][threadIdx.x] = w;
+        }
+      }
+      __syncthreads();
+      F2 acc[G][Op::NA];
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<F2>::zero();
+      if (expand) {
+#pragma unroll kSourceUnroll
+        for (int jj = 0; jj < TPB; ++jj) {
+          F2 s[2 * NU];
+#pragma unroll
+          for (int q = 0; q < NU; ++q) {
+            const Unit<F2> w = sm[q][jj];
+            s[2 * q] = w.a;
+            s[2 * q + 1] = w.b;
+          }
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            F2 arg = fma(yt[g][2], s[2], s[3]);  // |x|^2 - 2 y.x
+            arg = fma(yt[g][1], s[1], arg);
+            arg = fma(yt[g][0], s[0], arg);
+            Op::accumulate(tx[g], VT<F2>::expneg(arg), s + 4, acc[g]);
+          }
+        }
+      } else {
+#pragma unroll kSourceUnroll
+        for (int jj = 0; jj < TPB; ++jj) {
+          F2 s[2 * NU];
+#pragma unroll
+          for (int q = 0; q < NU; ++q) {
+            const Unit<F2> w = sm[q][jj];
+            s[2 * q] = w.a;
+            s[2 * q + 1] = w.b;
+          }
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const F2 d0 = yt[g][0] - s[0], d1 = yt[g][1] - s[1], d2 = yt[g][2] - s[2];
+            Op::accumulate(tx[g], VT<F2>::expneg(fma(d2, d2, fma(d1, d1, d0 * d0))), s + 4, acc[g]);
+          }
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int c = 0; c < Op::NA; ++c) {
+          if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * Op::NA + c, threadIdx.x);
+          cmp[g][c].merge(acc[g][c]);
+          if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
+        }
+      __syncthreads();
+    }
+
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const int i = base + (g * L + k) * TPB;
+        if (i < n) {
+          double fac = 1.0;
+          if (expand) {
+            double y2 = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const double yc = VT<F2>::lane(yt[g][c], k);
+              y2 += yc * yc;
+            }
+            fac = exp2(-y2);
+          }
+#pragma unroll
+          for (int c = 0; c < Op::NA; ++c) {
+            if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * Op::NA + c, threadIdx.x);
+            const float2 p = cmp[g][c].partial(k);
+            const double v = ((double)p.x + (double)p.y) * fac;
+            const float h = (float)v;
+            ws[((size_t)slot * Op::NA + c) * (size_t)n + i] = make_float2(h, (float)(v - (double)h));
+          }
+        }
+      }
+    u += j1 - j0;
+  }
+}
+
 // Coordinate boxes for exact culling, from the same scaled coordinates the pair kernel uses: block b < gx covers
 // target block b (its TPB * RT targets), block gx + j source tile j. boxes[6 b ..] = (lo xyz, hi xyz).
 template <class Op, typename V, int TPB, int RT>
@@ -584,7 +829,12 @@ template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline int ctas_per_sm() {
   static int cached = 0;
   if (cached == 0) {
-    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel<Op, V, TPB, RT, Fam>), TPB);
+    const void* k;
+    if constexpr (kUseExpanded<Op, V, Fam>)
+      k = reinterpret_cast<const void*>(&pairs_kernel_x<Op, TPB, kRunRT<Op, V, RT, Fam>>);
+    else
+      k = reinterpret_cast<const void*>(&pairs_kernel<Op, V, TPB, RT, Fam>);
+    int c = resident_ctas(k, TPB);
     cached = c > 0 ? c : 4;
   }
   return cached;
@@ -595,27 +845,34 @@ inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* w
                      cudaStream_t stream) {
   if (n <= 0) return kOk;
   if (n > INT32_MAX / 4 || m > INT32_MAX / 4) return kInvalidArgument;
-  SKPlan plan = make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial),
-                                   ctas_per_sm<Op, V, TPB, RT, Fam>());
+  constexpr int R = kRunRT<Op, V, RT, Fam>;
+  SKPlan plan = make_plan<TPB, R>(n, m, Op::NA, sizeof(typename VT<V>::Partial),
+                                  ctas_per_sm<Op, V, TPB, RT, Fam>());
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (plan.ws_bytes > 0 && ws == nullptr) return kInvalidArgument;
   auto* part = reinterpret_cast<typename VT<V>::Partial*>(ws);
   if (plan.W > 0) {
     float* boxes = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.box_off);
     if (Culled<Op>::value)
-      box_kernel<Op, V, TPB, RT><<<plan.gx + plan.TT, TPB, 0, stream>>>(P, (int)n, (int)m, plan.gx, boxes);
-    pairs_kernel<Op, V, TPB, RT, Fam><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C,
-                                                                   part, boxes);
+      box_kernel<Op, V, TPB, R><<<plan.gx + plan.TT, TPB, 0, stream>>>(P, (int)n, (int)m, plan.gx, boxes);
+    if constexpr (kUseExpanded<Op, V, Fam>) {
+      pairs_kernel_x<Op, TPB, R><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C, part,
+                                                              boxes);
+    } else {
+      pairs_kernel<Op, V, TPB, RT, Fam><<<plan.C, TPB, 0, stream>>>(P, (int)n, (int)m, plan.TT, plan.W, plan.C,
+                                                                     part, boxes);
+    }
   }
   const int fb = 256;
-  finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, TPB * RT, plan.TT, plan.W, plan.C,
+  finalize_kernel<Op, V><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, TPB * R, plan.TT, plan.W, plan.C,
                                                                       part);
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
 template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline size_t pairs_ws_bytes(int64_t n, int64_t m) {
-  return make_plan<TPB, RT>(n, m, Op::NA, sizeof(typename VT<V>::Partial), ctas_per_sm<Op, V, TPB, RT, Fam>())
+  return make_plan<TPB, kRunRT<Op, V, RT, Fam>>(n, m, Op::NA, sizeof(typename VT<V>::Partial),
+                                                ctas_per_sm<Op, V, TPB, RT, Fam>())
       .ws_bytes;
 }
 

@@ -71,6 +71,7 @@ struct OpSOFwd {
 // outputs px_prev, pa_prev are indexed by the local target index.
 struct OpSOBwd {
   static constexpr int NS = 12, NA = 12;
+  static constexpr int kMinCtas = LDDMM_SOBWD_MIN_CTAS;
   struct Params {
     const double *x, *a, *px, *pa;
     double *px_prev, *pa_prev;
@@ -155,6 +156,7 @@ struct OpSOBwd {
 // Accumulators: A = sum e c d (3), Q = sum e q_l (3). 19 FP32 + 1 SFU per pair.
 struct OpFOBwd {
   static constexpr int NS = 9, NA = 6;
+  static constexpr int kMinCtas = LDDMM_FOBWD_MIN_CTAS;
   static constexpr bool kCompInRegisters = true;  // measured faster than shared memory for this op
   struct Params {
     const double *x, *a, *p;

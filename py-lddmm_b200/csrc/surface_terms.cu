@@ -130,6 +130,49 @@ struct OpSurfEnergy {
       acc[2] = fma(e, s[6], acc[2]);
     }
   }
+  // Expanded-distance form (pairs_kernel_x). Payload: varifold (aw * factor, unit normal), measure
+  // (aw * factor), current (fw * surfel * factor). Varifold: 9 FP32 + 1 SFU per pair.
+  static constexpr bool kExpand = true;
+  static constexpr int NP = (KIND == LDDMM_DATA_VARIFOLD) ? 4 : (KIND == LDDMM_DATA_MEASURE ? 1 : 3);
+  template <typename V> struct TgtX { V n0, n1, n2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target_x(const Params& P, int i0, int i1, TgtX<V>& t) {
+    if (KIND == LDDMM_DATA_VARIFOLD) {
+      const FaceRec &r0 = P.T[i0], &r1 = P.T[i1];
+      t.n0 = VT<V>::pack(r0.n[0], r1.n[0]);
+      t.n1 = VT<V>::pack(r0.n[1], r1.n[1]);
+      t.n2 = VT<V>::pack(r0.n[2], r1.n[2]);
+    }
+  }
+  static __device__ __forceinline__ void target_point(const Params& P, int i, double* c) {
+    const FaceRec& r = P.T[i];
+    c[0] = r.c[0]; c[1] = r.c[1]; c[2] = r.c[2];
+  }
+  static __device__ __forceinline__ void source_point(const Params& P, int l, double* c, double* f) {
+    double fac;
+    const FaceRec& r = src_face(P.S, l, fac);
+    c[0] = r.c[0]; c[1] = r.c[1]; c[2] = r.c[2];
+    if (KIND == LDDMM_DATA_CURRENT) {
+      for (int k = 0; k < 3; ++k) f[k] = fac * r.s[k] * r.fw;
+    } else {
+      f[0] = fac * r.aw;
+      if (KIND == LDDMM_DATA_VARIFOLD)
+        for (int k = 0; k < 3; ++k) f[1 + k] = r.n[k];
+    }
+  }
+  template <typename V>
+  static __device__ __forceinline__ void accumulate(const TgtX<V>& t, V e, const V* s, V* acc) {
+    if (KIND == LDDMM_DATA_VARIFOLD) {
+      const V g = dot3(t.n0, t.n1, t.n2, s[1], s[2], s[3]);
+      acc[0] = fma(e * s[0], fma(g, g, VT<V>::dup(1.0)), acc[0]);
+    } else if (KIND == LDDMM_DATA_MEASURE) {
+      acc[0] = fma(e, s[0], acc[0]);
+    } else {
+      acc[0] = fma(e, s[0], acc[0]);
+      acc[1] = fma(e, s[1], acc[1]);
+      acc[2] = fma(e, s[2], acc[2]);
+    }
+  }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const FaceRec& r = P.T[i];
     if (KIND == LDDMM_DATA_CURRENT)
@@ -149,6 +192,7 @@ struct FaceGrad {
 template <int KIND>
 struct OpSurfGrad {
   static constexpr int NS = 7, NA = (KIND == LDDMM_DATA_VARIFOLD) ? 8 : (KIND == LDDMM_DATA_CURRENT ? 6 : 4);
+  static constexpr int kMinCtas = LDDMM_SURFGRAD_MIN_CTAS;
   static constexpr bool kCull = true;  // exact culling of far face tiles
   struct Params {
     const FaceRec* T;
