@@ -157,15 +157,24 @@ class Workspace:
 WORKSPACE = Workspace()
 
 
+_WS_BYTES = {}   # (entry, n, m, precision, device) -> bytes: the library's answer depends on nothing else
+
+
+def _ws_bytes(entry, n, m, precision):
+    key = (entry, int(n), int(m), int(precision), torch.cuda.current_device())
+    nb = _WS_BYTES.get(key)
+    if nb is None:
+        nb = _WS_BYTES[key] = getattr(lib(), entry)(key[1], key[2], key[3])
+    return nb
+
+
 def workspace(n, m, precision=FP32C):
-    nb = lib().lddmm_workspace_bytes(int(n), int(m), int(precision))
-    buf = WORKSPACE.get(nb)
+    buf = WORKSPACE.get(_ws_bytes('lddmm_workspace_bytes', n, m, precision))
     return ctypes.c_void_p(buf.data_ptr()), ctypes.c_size_t(buf.numel())
 
 
 def surface_workspace(nf, nf1, precision=FP32C):
-    nb = lib().lddmm_surface_workspace_bytes(int(nf), int(nf1), int(precision))
-    buf = WORKSPACE.get(nb)
+    buf = WORKSPACE.get(_ws_bytes('lddmm_surface_workspace_bytes', nf, nf1, precision))
     return ctypes.c_void_p(buf.data_ptr()), ctypes.c_size_t(buf.numel())
 
 

@@ -30,6 +30,9 @@ def _is_np(v):
     return not isinstance(v, torch.Tensor)
 
 
+_NO_ORIGIN = object()   # marks calls whose kernel needs no coordinate origin
+
+
 def _out(t, like_numpy):
     return nat.to_host(t) if like_numpy else t
 
@@ -126,7 +129,10 @@ class Kernel(KernelSpec):
         squeeze = A.dim() == 1
         if squeeze:
             A = A[:, None]
-        origin = nat.centroid(x)
+        # The Gaussian sums run the expanded-distance kernel (FP32) or FP64 arithmetic, both of which take coordinates
+        # relative to each target block's own centre in FP64: no origin is needed, and the host pass that computes one
+        # is skipped. The Laplacian FP32 kernel evaluates differences of origin-centred FP32 coordinates.
+        origin = _NO_ORIGIN if self.code == nat.KERNEL_GAUSS else nat.centroid(x)
         if A.shape[1] != 3:
             r = self._multi(lambda s: self._k_generic(Y, X, A, s, origin))
         else:
@@ -139,7 +145,7 @@ class Kernel(KernelSpec):
         n, m = Y.shape[0], X.shape[0]
         out = torch.empty((n, 3), dtype=torch.float64, device=Y.device)
         ws, wsb = nat.workspace(n, m, self.precision)
-        o = nat.origin_arg(origin if origin is not None else nat.centroid(X))
+        o = None if origin is _NO_ORIGIN else nat.origin_arg(origin if origin is not None else nat.centroid(X))
         nat.check(nat.lib().lddmm_apply_k(nat.ptr(Y), n, nat.ptr(X), nat.ptr(A), m, float(sigma), self.code, o,
                                           nat.ptr(out), self.precision, ws, wsb, nat.stream_ptr()), 'applyK')
         return out

@@ -29,6 +29,9 @@
 #define LDDMM_MIN_CTAS 1  // minimum resident CTAs per SM requested from ptxas (caps registers when > 1)
 #endif
 // per-op minimum resident CTAs (1: no register cap beyond the op's needs)
+#ifndef LDDMM_SOFWD_MIN_CTAS
+#define LDDMM_SOFWD_MIN_CTAS 4
+#endif
 #ifndef LDDMM_SOBWD_MIN_CTAS
 #define LDDMM_SOBWD_MIN_CTAS 4  // 124 registers, 4 CTAs per SM: 1.8% faster than 132 and 3 (A/B at level 6)
 #endif

@@ -13,7 +13,7 @@ namespace lddmm {
 // sharded step), sources all m rows; outputs x1, a1 are indexed by the local target index.
 struct OpSOFwd {
   static constexpr int NS = 6, NA = 6;
-  static constexpr int kMinCtas = 4;  // <= 128 registers at 128 threads: 16 warps per SM
+  static constexpr int kMinCtas = LDDMM_SOFWD_MIN_CTAS;  // 4: <= 128 registers at 128 threads, 16 warps per SM
   struct Params {
     const double *x, *a;
     double *x1, *a1;
