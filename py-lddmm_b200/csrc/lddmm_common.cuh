@@ -17,6 +17,8 @@
 // (compensated accumulation across tiles). Chunk partials are reduced in FP64, in fixed order, by the epilogue
 // kernel, which applies the per-target constants and writes float64 outputs (and, for shooting steps, the
 // float64 Euler update of the state).
+// Ops whose sum needs no coordinate differences (K a, the surface energies) run pairs_kernel_x instead: the
+// squared distance expanded about the centre of each target block, three packed FMAs per pair (see there).
 // FP64 path (the faithful baseline): the same pair functors instantiated with double, exp() and FP64 sums.
 #pragma once
 #include <cuda_runtime.h>

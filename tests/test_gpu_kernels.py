@@ -169,6 +169,30 @@ def test_diffk_options_and_fd_probe():
     assert abs(fd - an) < 1e-5 * max(1.0, abs(an))
 
 
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+def test_nan_propagates(dtype):
+    """As in the reference (numpy arithmetic), a NaN coordinate or momentum reaches every sum it enters: a NaN source
+    point or momentum makes every output NaN, a NaN target point only its own row (every exponential path, the
+    FMA-pipe one included)."""
+    from base.syntheticShapes import icosphere
+    x, _ = icosphere(4)
+    a = np.random.default_rng(4).normal(size=x.shape)
+    K = kernel(0.5, dtype)
+    xs = x.copy()
+    xs[17, 1] = np.nan
+    assert np.isnan(K.applyK(xs, a)).all()
+    an = a.copy()
+    an[5, 0] = np.nan
+    assert np.isnan(K.applyK(x, an)[:, 0]).all()
+    y = x[:1000].copy()
+    y[::7, 2] = np.nan
+    out = K.applyK(x, a, firstVar=y)
+    assert np.isnan(out[::7]).all()
+    rest = np.ones(y.shape[0], bool)
+    rest[::7] = False
+    assert np.isfinite(out[rest]).all()
+
+
 def test_errors_are_loud():
     from base.kernelFunctions import Kernel
     from base._native import LddmmError
