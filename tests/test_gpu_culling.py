@@ -60,16 +60,19 @@ def test_culled_shooting_and_laplacian_match_the_oracle():
     assert rel_err(KL.applyK(x0, a), O.laplacian.apply_k(x0, x0, a, 0.005, 3)) < 2e-5
 
 
-def test_culled_varifold_matches_the_oracle():
+@pytest.mark.parametrize('level,sigma', [(4, 0.05), (5, 0.1)])
+def test_culled_varifold_matches_the_oracle(level, sigma):
+    """Level 4 at sigma 0.05: face blocks too wide for the expanded-distance energy kernel (difference form);
+    level 5 at sigma 0.1: expanded form, with the tile pairs farther apart than 1.3 culled."""
     import oracle as O
     from base.surfaceDistances import SurfaceDataTerm
     from base.syntheticShapes import icosphere, bumpy_ellipsoid
-    x0, F = icosphere(4)
+    x0, F = icosphere(level)
     x1 = bumpy_ellipsoid(x0, seed=0)
-    Kd = kernel(0.05, 'float32')
+    Kd = kernel(sigma, 'float32')
     term = SurfaceDataTerm(F, x1, F, Kd, kind='varifold')
     e = float(term.energy(x0)[0])
-    e_ref = O.varifold_norm_def(x0, F, x1, F, 0.05)
+    e_ref = O.varifold_norm_def(x0, F, x1, F, sigma)
     assert abs(e - e_ref) < 1e-6 * abs(e_ref)
     g = term.gradient(x0).cpu().numpy()
-    assert rel_err(g, O.varifold_norm_gradient(x0, F, x1, F, 0.05)) < 2e-5
+    assert rel_err(g, O.varifold_norm_gradient(x0, F, x1, F, sigma)) < 2e-5
