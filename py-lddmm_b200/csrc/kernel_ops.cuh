@@ -66,11 +66,12 @@ struct OpK {
     c[0] = P.x[3 * l]; c[1] = P.x[3 * l + 1]; c[2] = P.x[3 * l + 2];
     f[0] = P.a[3 * l]; f[1] = P.a[3 * l + 1]; f[2] = P.a[3 * l + 2];
   }
-  template <typename V>
-  static __device__ __forceinline__ void accumulate(const TgtX<V>&, V e, const V* s, V* acc) {
-    acc[0] = fma(e, s[0], acc[0]);
-    acc[1] = fma(e, s[1], acc[1]);
-    acc[2] = fma(e, s[2], acc[2]);
+  // s: the staged source record (coordinates 0-2, |x|^2 3, payload from 4)
+  template <bool X, typename V>
+  static __device__ __forceinline__ void accumulate(const TgtX<V>&, const V*, V e, const V* s, V* acc) {
+    acc[0] = fma(e, s[4], acc[0]);
+    acc[1] = fma(e, s[5], acc[1]);
+    acc[2] = fma(e, s[6], acc[2]);
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     if (P.dots)

@@ -52,6 +52,9 @@
 #ifndef LDDMM_EXPAND
 #define LDDMM_EXPAND 1  // 0: the Gaussian sums of ops with an expanded-distance form use the difference form
 #endif
+#ifndef LDDMM_SOFWD_EXPAND
+#define LDDMM_SOFWD_EXPAND 1  // 0: the second-order forward step keeps the difference form
+#endif
 #ifndef LDDMM_SOURCE_UNROLL
 #define LDDMM_SOURCE_UNROLL 4  // unroll depth of the per-source loop over a shared-memory tile
 #endif
@@ -433,8 +436,19 @@ constexpr bool kUseExpanded = Expanded<Op>::value && std::is_same<V, F2>::value 
 #define LDDMM_X_COMP_SMEM 1  // 0: pairs_kernel_x keeps its compensated sums in registers
 #endif
 // Targets per thread of the kernel that runs an op (the plan, the launch and the epilogue all use it).
+// Optional members of an expanded op: kRtX (its targets per thread, default LDDMM_RT_X), NAX (accumulators of the
+// expanded form, default NA) with x_partial(expand, y, sums, out) mapping them to the NA sums the epilogue reads,
+// and kExpandR2 (its bound on a block's radius^2, default kExpandR2 below).
+template <class Op, class = void>
+struct RtXOf : std::integral_constant<int, LDDMM_RT_X> {};
+template <class Op>
+struct RtXOf<Op, std::void_t<decltype(Op::kRtX)>> : std::integral_constant<int, Op::kRtX> {};
+template <class Op, class = void>
+struct NAXOf : std::integral_constant<int, Op::NA> {};
+template <class Op>
+struct NAXOf<Op, std::void_t<decltype(Op::NAX)>> : std::integral_constant<int, Op::NAX> {};
 template <class Op, typename V, int RT, class Fam>
-constexpr int kRunRT = (kUseExpanded<Op, V, Fam> && LDDMM_RT_X > 0) ? LDDMM_RT_X : RT;
+constexpr int kRunRT = (kUseExpanded<Op, V, Fam> && RtXOf<Op>::value > 0) ? RtXOf<Op>::value : RT;
 
 template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 __global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
@@ -570,6 +584,18 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
 // drew such blocks). Both forms share the launch plan and the epilogue of pairs_kernel.
 // ---------------------------------------------------------------------------------------------------------
 constexpr float kExpandR2 = 64.0f;
+template <class Op, class = void>
+struct ExpandR2Of {
+  static constexpr float value = kExpandR2;
+};
+template <class Op>
+struct ExpandR2Of<Op, std::void_t<decltype(Op::kExpandR2)>> {
+  static constexpr float value = Op::kExpandR2;
+};
+template <class Op, class = void>
+struct HasXPartial : std::false_type {};
+template <class Op>
+struct HasXPartial<Op, std::void_t<decltype(&Op::x_partial)>> : std::true_type {};
 
 template <class Op, int TPB, int RT>
 __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
@@ -579,11 +605,12 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
   constexpr int G = RT / L;
   constexpr int NF = 4 + Op::NP;  // staged fields: X or x (3), q (1), payload (NP)
   constexpr int NU = (NF + 1) / 2;
+  constexpr int NAX = NAXOf<Op>::value;  // accumulators of the expanded form
   static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
   __shared__ Unit<F2> sm[NU][TPB];
   __shared__ float red[6][TPB / 32];
   constexpr bool kSm = LDDMM_X_COMP_SMEM != 0;
-  __shared__ F2 cs[kSm ? G * Op::NA * 2 : 1][TPB];
+  __shared__ F2 cs[kSm ? G * NAX * 2 : 1][TPB];
   const Frame& f = P.f;
   const double fo[3] = {f.o0, f.o1, f.o2};
   const int gx = (n + TPB * RT - 1) / (TPB * RT);
@@ -620,11 +647,11 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
       const float h = 0.5f * (hi[c] - lo[c]);
       rb2 = fmaf(h, h, rb2);
     }
-    const bool expand = rb2 <= kExpandR2;  // uniform over the CTA
+    const bool expand = rb2 <= ExpandR2Of<Op>::value;  // uniform over the CTA
 
     F2 yt[G][3];  // relative scaled target coordinates, lanes = targets (g L, g L + 1) of the thread
     typename Op::template TgtX<F2> tx[G];
-    Comp<F2> cmp[G][Op::NA];
+    Comp<F2> cmp[G][NAX];
 #pragma unroll
     for (int g = 0; g < G; ++g) {
       int i0 = base + (g * L) * TPB, i1 = base + (g * L + 1) * TPB;
@@ -638,9 +665,9 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
         yt[g][c] = f2((float)((y0[c] - fo[c]) * f.s - (double)ob[c]), (float)((y1[c] - fo[c]) * f.s - (double)ob[c]));
       Op::template load_target_x<F2>(P, i0, i1, tx[g]);
 #pragma unroll
-      for (int c = 0; c < Op::NA; ++c) {
+      for (int c = 0; c < NAX; ++c) {
         cmp[g][c].zero();
-        if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
+        if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * NAX + c, threadIdx.x);
       }
     }
 
@@ -676,11 +703,11 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
         }
       }
       __syncthreads();
-      F2 acc[G][Op::NA];
+      F2 acc[G][NAX];
 #pragma unroll
       for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<F2>::zero();
+        for (int c = 0; c < NAX; ++c) acc[g][c] = VT<F2>::zero();
       if (expand) {
 #pragma unroll kSourceUnroll
         for (int jj = 0; jj < TPB; ++jj) {
@@ -696,7 +723,7 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
             F2 arg = fma(yt[g][2], s[2], s[3]);  // |x|^2 - 2 y.x
             arg = fma(yt[g][1], s[1], arg);
             arg = fma(yt[g][0], s[0], arg);
-            Op::accumulate(tx[g], VT<F2>::expneg(arg), s + 4, acc[g]);
+            Op::template accumulate<true>(tx[g], yt[g], VT<F2>::expneg(arg), s, acc[g]);
           }
         }
       } else {
@@ -712,17 +739,17 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
 #pragma unroll
           for (int g = 0; g < G; ++g) {
             const F2 d0 = yt[g][0] - s[0], d1 = yt[g][1] - s[1], d2 = yt[g][2] - s[2];
-            Op::accumulate(tx[g], VT<F2>::expneg(fma(d2, d2, fma(d1, d1, d0 * d0))), s + 4, acc[g]);
+            Op::template accumulate<false>(tx[g], yt[g], VT<F2>::expneg(fma(d2, d2, fma(d1, d1, d0 * d0))), s, acc[g]);
           }
         }
       }
 #pragma unroll
       for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int c = 0; c < Op::NA; ++c) {
-          if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * Op::NA + c, threadIdx.x);
+        for (int c = 0; c < NAX; ++c) {
+          if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * NAX + c, threadIdx.x);
           cmp[g][c].merge(acc[g][c]);
-          if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * Op::NA + c, threadIdx.x);
+          if constexpr (kSm) cmp[g][c].template store<TPB>(cs, g * NAX + c, threadIdx.x);
         }
       __syncthreads();
     }
@@ -733,23 +760,31 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
       for (int k = 0; k < L; ++k) {
         const int i = base + (g * L + k) * TPB;
         if (i < n) {
-          double fac = 1.0;
-          if (expand) {
-            double y2 = 0.0;
+          double yr[3], y2 = 0.0;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              const double yc = VT<F2>::lane(yt[g][c], k);
-              y2 += yc * yc;
-            }
-            fac = exp2(-y2);
+          for (int c = 0; c < 3; ++c) {
+            yr[c] = VT<F2>::lane(yt[g][c], k);
+            y2 += yr[c] * yr[c];
+          }
+          const double fac = expand ? exp2(-y2) : 1.0;
+          double v[NAX], o[Op::NA];
+#pragma unroll
+          for (int c = 0; c < NAX; ++c) {
+            if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * NAX + c, threadIdx.x);
+            const float2 p = cmp[g][c].partial(k);
+            v[c] = (double)p.x + (double)p.y;
+          }
+          if constexpr (HasXPartial<Op>::value) {
+            Op::x_partial(expand, yr, v, o);
+          } else {
+#pragma unroll
+            for (int c = 0; c < Op::NA; ++c) o[c] = v[c];
           }
 #pragma unroll
           for (int c = 0; c < Op::NA; ++c) {
-            if constexpr (kSm) cmp[g][c].template load<TPB>(cs, g * Op::NA + c, threadIdx.x);
-            const float2 p = cmp[g][c].partial(k);
-            const double v = ((double)p.x + (double)p.y) * fac;
-            const float h = (float)v;
-            ws[((size_t)slot * Op::NA + c) * (size_t)n + i] = make_float2(h, (float)(v - (double)h));
+            const double w = o[c] * fac;
+            const float h = (float)w;
+            ws[((size_t)slot * Op::NA + c) * (size_t)n + i] = make_float2(h, (float)(w - (double)h));
           }
         }
       }

@@ -49,6 +49,59 @@ struct OpSOFwd {
     acc[4] = fma(ec, d1, acc[4]);
     acc[5] = fma(ec, d2, acc[5]);
   }
+  // Expanded-distance form (pairs_kernel_x, Gaussian FP32): with c = a_k.a_l, the sum of e c (y - x) is written
+  // y S - sum e c x with S = sum e c, and the staged X = -2 x gives sum e c x = -E/2 for E = sum e c X; no
+  // difference y - x is formed (14 FP32 + 1 SFU per pair). Blocks too wide for that form (difference form) sum
+  // e c (y - x) directly, without the cancellation. Radius^2 bound 32: the cancellation in y S - sum e c x grows
+  // with the block radius (FP32 emulation, targets in a ball of radius^2 16: 3.7e-7 relative, against 1.2e-7 for
+  // the difference form; 4.6e-7 at 64).
+  static constexpr bool kExpand = LDDMM_SOFWD_EXPAND != 0;
+  static constexpr int NP = 3, NAX = 7, kRtX = 4;
+  static constexpr float kExpandR2 = 32.0f;
+  template <typename V> struct TgtX { V a0, a1, a2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target_x(const Params& P, int i0, int i1, TgtX<V>& t) {
+    i0 += P.row0;
+    i1 += P.row0;
+    t.a0 = tgt_field<V>(P.a, 3, i0, i1, 0);
+    t.a1 = tgt_field<V>(P.a, 3, i0, i1, 1);
+    t.a2 = tgt_field<V>(P.a, 3, i0, i1, 2);
+  }
+  static __device__ __forceinline__ void target_point(const Params& P, int i, double* c) {
+    const int g = P.row0 + i;
+    c[0] = P.x[3 * g]; c[1] = P.x[3 * g + 1]; c[2] = P.x[3 * g + 2];
+  }
+  static __device__ __forceinline__ void source_point(const Params& P, int l, double* c, double* f) {
+    for (int k = 0; k < 3; ++k) {
+      c[k] = P.x[3 * l + k];
+      f[k] = P.a[3 * l + k];
+    }
+  }
+  // s: the staged source record (X or x 0-2, |x|^2 3, a 4-6); y: the target pair's relative coordinates.
+  // Sums: K a (0-2); expanded: S (3), E (4-6); difference form: sum e c d (4-6).
+  template <bool X, typename V>
+  static __device__ __forceinline__ void accumulate(const TgtX<V>& t, const V* y, V e, const V* s, V* acc) {
+    acc[0] = fma(e, s[4], acc[0]);
+    acc[1] = fma(e, s[5], acc[1]);
+    acc[2] = fma(e, s[6], acc[2]);
+    const V ec = e * dot3(t.a0, t.a1, t.a2, s[4], s[5], s[6]);
+    if constexpr (X) {
+      acc[3] = acc[3] + ec;
+      acc[4] = fma(ec, s[0], acc[4]);
+      acc[5] = fma(ec, s[1], acc[5]);
+      acc[6] = fma(ec, s[2], acc[6]);
+    } else {
+      acc[4] = fma(ec, y[0] - s[0], acc[4]);
+      acc[5] = fma(ec, y[1] - s[1], acc[5]);
+      acc[6] = fma(ec, y[2] - s[2], acc[6]);
+    }
+  }
+  static __device__ __forceinline__ void x_partial(bool expand, const double* y, const double* v, double* o) {
+    for (int c = 0; c < 3; ++c) {
+      o[c] = v[c];
+      o[3 + c] = expand ? y[c] * v[3] + 0.5 * v[4 + c] : v[4 + c];
+    }
+  }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const double ka = P.dt * P.f.kappa;
     const int g = P.row0 + i;

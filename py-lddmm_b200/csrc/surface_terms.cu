@@ -160,17 +160,18 @@ struct OpSurfEnergy {
         for (int k = 0; k < 3; ++k) f[1 + k] = r.n[k];
     }
   }
-  template <typename V>
-  static __device__ __forceinline__ void accumulate(const TgtX<V>& t, V e, const V* s, V* acc) {
+  template <bool X, typename V>
+  static __device__ __forceinline__ void accumulate(const TgtX<V>& t, const V*, V e, const V* s, V* acc) {
+    const V* w = s + 4;  // the payload of the staged record
     if (KIND == LDDMM_DATA_VARIFOLD) {
-      const V g = dot3(t.n0, t.n1, t.n2, s[1], s[2], s[3]);
-      acc[0] = fma(e * s[0], fma(g, g, VT<V>::dup(1.0)), acc[0]);
+      const V g = dot3(t.n0, t.n1, t.n2, w[1], w[2], w[3]);
+      acc[0] = fma(e * w[0], fma(g, g, VT<V>::dup(1.0)), acc[0]);
     } else if (KIND == LDDMM_DATA_MEASURE) {
-      acc[0] = fma(e, s[0], acc[0]);
+      acc[0] = fma(e, w[0], acc[0]);
     } else {
-      acc[0] = fma(e, s[0], acc[0]);
-      acc[1] = fma(e, s[1], acc[1]);
-      acc[2] = fma(e, s[2], acc[2]);
+      acc[0] = fma(e, w[0], acc[0]);
+      acc[1] = fma(e, w[1], acc[1]);
+      acc[2] = fma(e, w[2], acc[2]);
     }
   }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
