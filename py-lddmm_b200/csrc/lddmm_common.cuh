@@ -55,6 +55,9 @@
 #ifndef LDDMM_SOFWD_EXPAND
 #define LDDMM_SOFWD_EXPAND 1  // 0: the second-order forward step keeps the difference form
 #endif
+#ifndef LDDMM_SURFGRAD_EXPAND
+#define LDDMM_SURFGRAD_EXPAND 1  // 0: the varifold and measure gradients keep the difference form
+#endif
 #ifndef LDDMM_SOURCE_UNROLL
 #define LDDMM_SOURCE_UNROLL 4  // unroll depth of the per-source loop over a shared-memory tile
 #endif

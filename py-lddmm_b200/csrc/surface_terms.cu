@@ -244,6 +244,79 @@ struct OpSurfGrad {
       acc[3] = fma(ea, d2, acc[3]);
     }
   }
+  // Expanded-distance form (pairs_kernel_x; varifold and measure): the centre term sum f (y - x) is written
+  // y S - sum f x with S = sum f, a sum these kinds accumulate anyway (varifold: f = e aw (1 + g^2), S in slot 7;
+  // measure: f = e aw, slot 0), and the staged X = -2 x gives sum f x = -E/2; no difference y - x is formed
+  // (varifold: 19 FP32 + 1 SFU per pair) and no accumulator or staged field is added. Blocks too wide for the form
+  // sum f (y - x) directly. Radius^2 bound 32, as for the second-order forward step.
+  static constexpr bool kExpand = LDDMM_SURFGRAD_EXPAND != 0 && KIND != LDDMM_DATA_CURRENT;
+  static constexpr int NP = (KIND == LDDMM_DATA_VARIFOLD) ? 4 : 1, kRtX = 4;
+  static constexpr float kExpandR2 = 32.0f;
+  template <typename V> struct TgtX { V n0, n1, n2; };
+  template <typename V>
+  static __device__ __forceinline__ void load_target_x(const Params& P, int i0, int i1, TgtX<V>& t) {
+    if (KIND == LDDMM_DATA_VARIFOLD) {
+      const FaceRec &r0 = P.T[i0], &r1 = P.T[i1];
+      t.n0 = VT<V>::pack(r0.n[0], r1.n[0]);
+      t.n1 = VT<V>::pack(r0.n[1], r1.n[1]);
+      t.n2 = VT<V>::pack(r0.n[2], r1.n[2]);
+    }
+  }
+  static __device__ __forceinline__ void target_point(const Params& P, int i, double* c) {
+    const FaceRec& r = P.T[i];
+    c[0] = r.c[0]; c[1] = r.c[1]; c[2] = r.c[2];
+  }
+  static __device__ __forceinline__ void source_point(const Params& P, int l, double* c, double* f) {
+    double fac;
+    const FaceRec& r = src_face(P.S, l, fac);
+    c[0] = r.c[0]; c[1] = r.c[1]; c[2] = r.c[2];
+    f[0] = fac * r.aw;
+    if (KIND == LDDMM_DATA_VARIFOLD)
+      for (int k = 0; k < 3; ++k) f[1 + k] = r.n[k];
+  }
+  // s: staged record (X or x 0-2, |x|^2 3, aw 4, unit normal 5-7)
+  template <bool X, typename V>
+  static __device__ __forceinline__ void accumulate(const TgtX<V>& t, const V* y, V e, const V* s, V* acc) {
+    const V ea = e * s[4];
+    if constexpr (KIND == LDDMM_DATA_VARIFOLD) {
+      const V g = dot3(t.n0, t.n1, t.n2, s[5], s[6], s[7]);
+      const V eag = ea * g;
+      const V eag2 = eag * g;
+      const V t2 = eag + eag;
+      acc[0] = fma(t2, s[5], acc[0]);
+      acc[1] = fma(t2, s[6], acc[1]);
+      acc[2] = fma(t2, s[7], acc[2]);
+      acc[3] = acc[3] + (ea - eag2);
+      const V eaf = ea + eag2;
+      if constexpr (X) {
+        acc[4] = fma(eaf, s[0], acc[4]);
+        acc[5] = fma(eaf, s[1], acc[5]);
+        acc[6] = fma(eaf, s[2], acc[6]);
+      } else {
+        acc[4] = fma(eaf, y[0] - s[0], acc[4]);
+        acc[5] = fma(eaf, y[1] - s[1], acc[5]);
+        acc[6] = fma(eaf, y[2] - s[2], acc[6]);
+      }
+      acc[7] = acc[7] + eaf;
+    } else {
+      acc[0] = acc[0] + ea;
+      if constexpr (X) {
+        acc[1] = fma(ea, s[0], acc[1]);
+        acc[2] = fma(ea, s[1], acc[2]);
+        acc[3] = fma(ea, s[2], acc[3]);
+      } else {
+        acc[1] = fma(ea, y[0] - s[0], acc[1]);
+        acc[2] = fma(ea, y[1] - s[1], acc[2]);
+        acc[3] = fma(ea, y[2] - s[2], acc[3]);
+      }
+    }
+  }
+  static __device__ __forceinline__ void x_partial(bool expand, const double* y, const double* v, double* o) {
+    for (int c = 0; c < NA; ++c) o[c] = v[c];
+    const int d = (KIND == LDDMM_DATA_VARIFOLD) ? 4 : 1, sum = (KIND == LDDMM_DATA_VARIFOLD) ? 7 : 0;
+    if (expand)
+      for (int c = 0; c < 3; ++c) o[d + c] = y[c] * v[sum] + 0.5 * v[d + c];
+  }
   static __device__ __forceinline__ void finalize(const Params& P, int i, const double* acc) {
     const FaceRec& r = P.T[i];
     FaceGrad g;
