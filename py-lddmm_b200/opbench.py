@@ -25,11 +25,12 @@ from base import _native as nat  # noqa: E402
 from base.surfaceDistances import vertex_face_table  # noqa: E402
 from base.syntheticShapes import icosphere, bumpy_ellipsoid  # noqa: E402
 
-# FP32 lane-ops and SFU ops per pair of each kernel (packed instructions counted per lane); applyK: its
-# expanded-distance form (blocks whose radius is too large for it take the 9-op difference form)
+# FP32 lane-ops and SFU ops per pair of each kernel (packed instructions counted per lane); applyK, the
+# second-order step and the varifold energy and gradient: their expanded-distance form (blocks whose radius is too
+# large for it take the difference form: 9, 16, 12 and 22)
 OPS = {'applyK': (6, 1), 'applyDiffKT_lddmm': (16, 1), 'applyDDiffK11and12': (23, 1), 'applyDiffK1and2': (16, 1),
-       'so_step': (16, 1), 'so_adjoint_step': (37, 1), 'fo_adjoint_step': (19, 1), 'varifold_energy': (13, 1),
-       'varifold_gradient': (22, 1)}
+       'so_step': (14, 1), 'so_adjoint_step': (37, 1), 'fo_adjoint_step': (19, 1), 'varifold_energy': (9, 1),
+       'varifold_gradient': (19, 1)}
 
 
 def main():
