@@ -9,8 +9,8 @@
  *    with the reference's default `ms_exponent = -1` weighting; multi-scale kernels are one call per width.
  *  - `origin` (host pointer to 3 doubles, may be NULL = 0): coordinates are centred on it before the FP32
  *    conversion. Results are translation invariant; pass the centroid of the points for best FP32 accuracy.
- *    The Gaussian kernel sum (lddmm_apply_k) and the surface energies in FP32 centre every target block on its
- *    own in FP64 and do not depend on it.
+ *    The Gaussian FP32 kernels of lddmm_apply_k, the second-order forward step, the surface energies and the
+ *    varifold / measure gradients centre every target block on its own in FP64 and do not depend on it.
  *  - `precision`: LDDMM_FP32C = FP32 pair arithmetic with compensated (two-sum) accumulation across tiles and
  *    FP64 epilogues; LDDMM_FP64 = the same kernels in FP64 (the faithful baseline).
  *  - `workspace` / `workspace_bytes`: caller-provided device scratch of at least
