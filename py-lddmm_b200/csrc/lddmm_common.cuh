@@ -407,6 +407,13 @@ struct MinCtas : std::integral_constant<int, LDDMM_MIN_CTAS> {};
 template <class Op>
 struct MinCtas<Op, F2, std::void_t<decltype(Op::kMinCtas)>> : std::integral_constant<int, Op::kMinCtas> {};
 
+// Ops may set their own unroll depth of the per-source loop (`static constexpr int kUnroll`); the default is
+// LDDMM_SOURCE_UNROLL.
+template <class Op, class = void>
+struct UnrollOf : std::integral_constant<int, kSourceUnroll> {};
+template <class Op>
+struct UnrollOf<Op, std::void_t<decltype(Op::kUnroll)>> : std::integral_constant<int, Op::kUnroll> {};
+
 // Ops whose sums are culled declare `static constexpr bool kCull = true;`: the surface data terms, whose faces are
 // stored in a spatially coherent order by mesh generators and whose widths are often small against the shape.
 // Elsewhere the box pre-pass and the per-tile test cost 2-3% and seldom pay (vertex orders are less coherent, and
@@ -460,6 +467,7 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
   constexpr int L = VT<V>::kLanes;
   constexpr int G = RT / L;  // lane groups per thread
   constexpr int NU = (Op::NS + 1) / 2;
+  constexpr int kUnroll = UnrollOf<Op>::value;
   static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
   __shared__ Unit<V> sm[NU][TPB];
   // The segment's compensated sums live in shared memory (one private column per thread: no barrier needed) unless
@@ -528,7 +536,7 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, V>::value)
       for (int g = 0; g < G; ++g)
 #pragma unroll
         for (int c = 0; c < Op::NA; ++c) acc[g][c] = VT<V>::zero();
-#pragma unroll kSourceUnroll
+#pragma unroll kUnroll
       for (int jj = 0; jj < TPB; ++jj) {
         V s[2 * NU];
 #pragma unroll
@@ -609,6 +617,7 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
   constexpr int NF = 4 + Op::NP;  // staged fields: X or x (3), q (1), payload (NP)
   constexpr int NU = (NF + 1) / 2;
   constexpr int NAX = NAXOf<Op>::value;  // accumulators of the expanded form
+  constexpr int kUnroll = UnrollOf<Op>::value;
   static_assert(RT % L == 0, "targets per thread must be a multiple of the lane count");
   __shared__ Unit<F2> sm[NU][TPB];
   __shared__ float red[6][TPB / 32];
@@ -712,7 +721,7 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
 #pragma unroll
         for (int c = 0; c < NAX; ++c) acc[g][c] = VT<F2>::zero();
       if (expand) {
-#pragma unroll kSourceUnroll
+#pragma unroll kUnroll
         for (int jj = 0; jj < TPB; ++jj) {
           F2 s[2 * NU];
 #pragma unroll
@@ -730,7 +739,7 @@ __global__ void __launch_bounds__(TPB, MinCtas<Op, F2>::value)
           }
         }
       } else {
-#pragma unroll kSourceUnroll
+#pragma unroll kUnroll
         for (int jj = 0; jj < TPB; ++jj) {
           F2 s[2 * NU];
 #pragma unroll

@@ -194,6 +194,7 @@ template <int KIND>
 struct OpSurfGrad {
   static constexpr int NS = 7, NA = (KIND == LDDMM_DATA_VARIFOLD) ? 8 : (KIND == LDDMM_DATA_CURRENT ? 6 : 4);
   static constexpr int kMinCtas = LDDMM_SURFGRAD_MIN_CTAS;
+  static constexpr int kUnroll = 8;  // measured 1.9% faster than 4 (varifold, level 6)
   static constexpr bool kCull = true;  // exact culling of far face tiles
   struct Params {
     const FaceRec* T;
