@@ -101,8 +101,8 @@ int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m,
  * plugin host that gives its plugins no allocator, or a latency-critical path that may not call cudaMalloc because
  * it can synchronise the device). This entry point has no counterpart in the reference.
  * Its scratch is a 32 MiB array built into the library; every GPU that loads the library holds it until exit.
- * Limits: n <= 262,144 targets (any m); a request whose partial sums would not fit the array is rejected with
- * LDDMM_ERR_WORKSPACE before any launch. The first call on a device looks up the array's address with that device
+ * Limits: n <= 262,144 targets; with up to 75 million sources every such request fits, and a request whose scratch
+ * would not fit the array is rejected with LDDMM_ERR_WORKSPACE before any launch. The first call on a device looks up the array's address with that device
  * current: make it before any stream capture. All calls share the array (nothing needs clearing between calls);
  * calls that overlap on the GPU race on it and must be serialised by the caller. */
 int lddmm_apply_k_static(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,

@@ -8,9 +8,9 @@
 // library, which every GPU that loads the library holds (32 MiB) until the process exits.
 //
 // Limits and rules (repeated in include/lddmm_b200.h):
-//  - at most kStaticMaxTargets = 262,144 targets (any number of sources); with the shipped launch shapes every such
-//    problem fits the 32 MiB array, and a request whose partial sums would not fit is rejected before any launch
-//    with LDDMM_ERR_WORKSPACE;
+//  - at most kStaticMaxTargets = 262,144 targets; with the shipped launch shapes every such problem with up to 75
+//    million sources fits the 32 MiB array (the partial sums and the per-tile coordinate boxes), and a request that
+//    would not fit is rejected before any launch with LDDMM_ERR_WORKSPACE;
 //  - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
 //    current; make that first call before any stream capture on the device;
 //  - every call shares the one array and leaves its partial sums in it. Nothing needs clearing between calls: each
