@@ -35,7 +35,7 @@
 #define LDDMM_SOFWD_MIN_CTAS 4
 #endif
 #ifndef LDDMM_SOBWD_MIN_CTAS
-#define LDDMM_SOBWD_MIN_CTAS 4  // 124 registers, 4 CTAs per SM: 1.8% faster than 132 and 3 (A/B at level 6)
+#define LDDMM_SOBWD_MIN_CTAS 1  // at 4 targets per thread (LDDMM_RT_ADJOINT) no cap: 254 registers, 2 CTAs per SM
 #endif
 #ifndef LDDMM_FOBWD_MIN_CTAS
 #define LDDMM_FOBWD_MIN_CTAS 1

@@ -126,6 +126,7 @@ struct OpSOFwd {
 struct OpSOBwd {
   static constexpr int NS = 12, NA = 12;
   static constexpr int kMinCtas = LDDMM_SOBWD_MIN_CTAS;
+  static constexpr bool kCompInRegisters = true;  // with 4 targets per thread: measured faster than shared memory
   static constexpr int kUnroll = 8;  // measured 1.4% faster than 4 (level 6)
   struct Params {
     const double *x, *a, *px, *pa;
@@ -268,7 +269,8 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
   auto upd = [&](size_t v) { b = v > b ? v : b; };
   if (precision == kFP32Compensated) {
     upd(pairs_ws_bytes_any<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
-    upd(pairs_ws_bytes_any<OpSOBwd, F2, kTpbHeavy, kRtHeavy>(n, n));
+    upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtAdjoint, Gauss>(n, n));
+    upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtHeavy, Laplacian>(n, n));
     upd(pairs_ws_bytes_any<OpFOBwd, F2, kTpbLight, kRtLight>(n, n));
     upd(pairs_ws_bytes_any<OpK, F2, kTpbLight, kRtLight>(n, n));
   } else {
@@ -283,13 +285,15 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
 
 namespace {
 
-// Launch shapes per precision: light (forward / first-order) and heavy (second-order adjoint) ops.
+// Launch shapes per precision: light (forward / first-order) ops and the second-order adjoint step.
 template <typename V> struct Shape;
 template <> struct Shape<F2> {
-  static constexpr int kTpb = kTpbLight, kRt = kRtLight, kTpbH = kTpbHeavy, kRtH = kRtHeavy;
+  // the adjoint step: 4 targets per thread for the Gaussian, 2 for the Laplacian (whose radial profile needs the
+  // registers: 4 would spill)
+  static constexpr int kTpb = kTpbLight, kRt = kRtLight, kTpbH = kTpbHeavy, kRtH = kRtAdjoint, kRtHL = kRtHeavy;
 };
 template <> struct Shape<double> {
-  static constexpr int kTpb = kTpb64, kRt = kRt64, kTpbH = kTpb64, kRtH = kRt64;
+  static constexpr int kTpb = kTpb64, kRt = kRt64, kTpbH = kTpb64, kRtH = kRt64, kRtHL = kRt64;
 };
 
 template <typename V>
@@ -338,7 +342,9 @@ int so_adjoint_step(const double* x, const double* a, const double* px, const do
                     double dt, double* px_prev, double* pa_prev, void* ws, size_t wsb, cudaStream_t st,
                     int64_t row0 = 0, int64_t nrows = -1) {
   OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt, (int)row0};
-  return run_pairs_k<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
+  const int64_t rows = nrows < 0 ? n : nrows;
+  if (f.family == kGauss) return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH, Gauss>(P, rows, n, ws, wsb, st);
+  return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtHL, Laplacian>(P, rows, n, ws, wsb, st);
 }
 
 template <typename V>
