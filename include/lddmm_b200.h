@@ -101,9 +101,11 @@ int lddmm_apply_k_tensor(const double* y, int64_t n, const double* x, int64_t m,
  * plugin host that gives its plugins no allocator, or a latency-critical path that may not call cudaMalloc because
  * it can synchronise the device). This entry point has no counterpart in the reference.
  * Its scratch is a 32 MiB array built into the library; every GPU that loads the library holds it until exit.
- * Limits: n <= 262,144 targets; with up to 75 million sources every such request fits, and a request whose scratch
- * would not fit the array is rejected with LDDMM_ERR_WORKSPACE before any launch. The first call on a device looks up the array's address with that device
- * current: make it before any stream capture. All calls share the array (nothing needs clearing between calls);
+ * Limits: n <= 262,144 targets. The scratch is the sum's partial slots only and does not grow with the number of
+ * sources: on a B200 every request with at most 262,144 targets fits (20.7 MiB at most) for any source count up to
+ * the library's limit of 536,870,911. A request whose scratch would not fit the array (a device with many more
+ * resident CTAs) is rejected with LDDMM_ERR_WORKSPACE before any launch. The first call on a device looks up the
+ * array's address with that device current: make it before any stream capture. All calls share the array (nothing needs clearing between calls);
  * calls that overlap on the GPU race on it and must be serialised by the caller. */
 int lddmm_apply_k_static(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma,
                          const double* origin, double* out, int precision, lddmm_stream_t stream);

@@ -25,7 +25,7 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
          lineSearch='Weak_Wolfe'):
     for need in ('getVariable', 'objectiveFun', 'updateTry', 'acceptVarTry', 'getGradient'):
         if not hasattr(opt, need):
-            logging.error('Error: required functions are not provided')
+            logging.error('bfgs: the object lacks part of the optimiser protocol (%s)', need)
             return
     line_search = {'Wolfe': line_search_wolfe, 'Goldstein_Price': line_search_goldstein_price,
                    'Weak_Wolfe': line_search_weak_wolfe}.get(lineSearch, line_search_weak_wolfe)
@@ -53,7 +53,7 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
         opt.obj = None
     obj = opt.objectiveFun()
     opt.reset = False
-    logging.info('iteration 0: obj = {0: .5f}'.format(obj))
+    logging.info(f'bfgs start: objective {obj:.6g}')
 
     history = []
     it = 0
@@ -77,7 +77,7 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
             opt.obj = None
             obj = opt.objectiveFun()
             if verb:
-                logging.info(f'recomputed objective {obj:.5f}')
+                logging.info(f'bfgs restart: objective re-evaluated as {obj:.6g}')
             obj_old = None
             gval = None
         grd = opt.getGradient(gradCoeff) if gval is None else gval
@@ -88,7 +88,8 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
             o1 = opt.updateTry(dirfoo, epsfoo, obj - 1e8)
             o2 = opt.updateTry(dirfoo, -epsfoo, obj - 1e8)
             [gd] = dot(grd, [dirfoo])
-            logging.info('Test Gradient: %.4f %.4f' % ((o1 - o2) / (2 * epsfoo), -gd * gradCoeff))
+            logging.info(f'gradient check along a random direction: finite difference {(o1 - o2) / (2 * epsfoo):.4f}, '
+                         f'analytic {-gd * gradCoeff:.4f}')
 
         if not opt.reset and it > 0:
             history.append([diffVar, addProd(grd, grdOld, -1)])
@@ -129,7 +130,7 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
                 gradEps = max(0.001 * np.sqrt(grd2), 0.0001)
             else:
                 gradEps = min(gradEps, 0.0001 * np.sqrt(grd2))
-            logging.info(f'Gradient threshold: {gradEps:.6f}')
+            logging.info(f'bfgs: stop when the gradient norm falls below {gradEps:.6g}')
 
         if it < burnIn:
             Wolfe = False
@@ -148,9 +149,9 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
             obj = phi_star
             newreset = False
         else:
-            logging.info('Wolfe search unsuccessful')
+            logging.info('bfgs: the line search found no acceptable step')
             if opt.reset:
-                logging.info('Cannot go any further')
+                logging.info('bfgs: second failed line search in a row after a restart; stopping')
                 opt.converged = False
                 finish()
                 break
@@ -158,9 +159,9 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
             gval = None
 
         if obj_old is not None and np.fabs(obj - obj_old) < 1e-7 and stopCondition():
-            logging.info(f'iteration {it + 1:d}: obj = {obj:.5f}, eps = {eps:.5f}, gradient: {np.sqrt(grd2):.5f}')
+            logging.info(f'bfgs step {it + 1:d}: objective {obj:.6g}, step {eps:.4g}, |gradient| {np.sqrt(grd2):.4g}')
             if it > burnIn or opt.reset:
-                logging.info('Stopping Gradient Descent: small variation')
+                logging.info('bfgs: objective change below 1e-7; converged')
                 opt.converged = True
                 finish()
                 break
@@ -169,12 +170,12 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
         now = time.process_time()
         if verb or it == maxIter:
             e_s = 'None' if eps is None else f'{eps:.5f}'
-            logging.info(f'iteration {it + 1:d}: obj = {obj:.5f}, eps = {e_s}, gradient: {np.sqrt(grd2):.5f}, '
-                         f'time = {now - t0:.04f}, {now - t_iter:.04f}')
+            logging.info(f'bfgs step {it + 1:d}: objective {obj:.6g}, step {e_s}, |gradient| {np.sqrt(grd2):.4g}, '
+                         f'{now - t0:.3f} s')
         t_iter = now
 
         if np.sqrt(grd2) < gradEps and stopCondition():
-            logging.info('Stopping Gradient Descent: small gradient')
+            logging.info('bfgs: gradient norm below the threshold; converged')
             opt.converged = True
             finish()
             break

@@ -1,45 +1,47 @@
-"""Linear conjugate gradient used by `Kernel.solve` (reference: base/conjugateGradient.py:351-409).
+"""Linear conjugate gradient for `Kernel.solve` (the reference's `Kernel.solve` calls its own linearcg,
+base/kernelFunctions.py:676-680; same call signature, `linearcg(op, b, iterMax, x0, param, verb)`).
 
-Solves op(x) = b for a symmetric positive operator (the kernel sum a -> K(x) a runs on the GPU) with the
-reference's stopping rules: |r|^2 < 1e-10 at start, step alpha * mean|p| < 1e-10, or a relative change of the
-quadratic energy below 1e-20.
+Hestenes-Stiefel CG for op(x) = b with op symmetric positive definite (a -> K(x) a, whose kernel sums run on the
+GPU). It starts from x0 (zero by default) and stops when the residual norm |b - op(x)| falls to `tol` times |b|,
+when the curvature p.op(p) is no longer positive, or after iterMax operator applications. Arrays may be numpy
+arrays or torch tensors; inner products are read back as Python floats.
 """
 import logging
 
 import numpy as np
 
 
-def linearcg(op, b, iterMax=100, x0=None, param=None, verb=False):
-    apply = (lambda v: op(v)) if param is None else (lambda v: op(v, param))
-    x = np.zeros(np.shape(b)) if x0 is None else x0
-    z = apply(x) - 2 * b
-    ener = (z * x).sum()
-    old = ener
-    r = -z - b
-    mu = None
-    p = None
-    for i in range(iterMax):
-        if i == 0:
-            mu = (r * r).sum()
-            if mu < 1e-10:
-                return x
-            p = r
-        else:
-            mu_old = mu
-            mu = (r * r).sum()
-            p = r + (mu / mu_old) * p
+def _dot(u, v):
+    return float((u * v).sum())
+
+
+def linearcg(op, b, iterMax=100, x0=None, param=None, verb=False, tol=1e-10):
+    apply = op if param is None else (lambda v: op(v, param))
+    if x0 is None:
+        x = b * 0
+        r = b * 1
+    else:
+        x = x0 * 1
+        r = b - apply(x)
+    bnorm = np.sqrt(_dot(b, b))
+    if bnorm == 0.0:
+        return x
+    p = r * 1
+    rr = _dot(r, r)
+    for k in range(iterMax):
+        if np.sqrt(rr) <= tol * bnorm:
+            break
         q = apply(p)
-        alpha = mu / (p * q).sum()
-        x = x + alpha * p
-        r = r - alpha * q
-        z = z + alpha * q
-        ener = (z * x).sum()
-        if verb and i % 10 == 0:
-            logging.info('iter {0:d} ener = {1:.6f} error = {2:.15f}'.format(i + 1, float(ener),
-                                                                          float(((apply(x) - b) ** 2).sum())))
-        if alpha * np.mean(np.fabs(p)) < 1e-10:
-            return x
-        if np.fabs(ener - old) < 1e-20 * np.fabs(old):
-            return x
-        old = ener
+        curv = _dot(p, q)
+        if not curv > 0.0:
+            logging.info(f'linearcg: non-positive curvature {curv:.3e} at step {k}; returning the current iterate')
+            break
+        step = rr / curv
+        x = x + step * p
+        r = r - step * q
+        rr_next = _dot(r, r)
+        p = r + (rr_next / rr) * p
+        rr = rr_next
+        if verb:
+            logging.info(f'linearcg step {k + 1}: relative residual {np.sqrt(rr) / bnorm:.3e}')
     return x

@@ -300,7 +300,7 @@ class Kernel(KernelSpec):
         k1 = (p * self.applyK(x, a, firstVar=y + eps * dy)).sum()
         grd = self.applyDiffKT(x, p, a, firstVar=y)
         fd, an = float((k1 - k0) / eps), float((grd * dy).sum())
-        logging.info('test diffKT: {0:.5f}, {1:.5f}'.format(fd, an))
+        logging.info(f'applyDiffKT check: finite difference {fd:.5f}, analytic {an:.5f}')
         return fd, an
 
     def applyDivergence(self, x, a, firstVar=None):

@@ -63,7 +63,8 @@ def line_search_weak_wolfe(opt, pk, gfk=None, old_fval=None, old_old_fval=None, 
         it += 1
 
     if n_grad == maxiter:
-        logging.warning('Weak Wolfe condition: maximum gradient computations attained: switching to backtracking')
+        logging.warning(f'weak-Wolfe search: {maxiter} gradients spent without meeting the curvature test; '
+                        'halving the step until the decrease test holds')
         last_grad[0] = None
         while it < n_f_max:
             if f < old_fval + c1 * t * d0 * g:
@@ -74,7 +75,7 @@ def line_search_weak_wolfe(opt, pk, gfk=None, old_fval=None, old_old_fval=None, 
             it += 1
 
     if it == n_f_max:
-        logging.warning(f'Weak Wolfe condition: maximum number of iterations attained {f:.5f}--{old_fval:.5f}')
+        logging.warning(f'weak-Wolfe search gave up after {n_f_max} trial steps (objective {f:.6g} against {old_fval:.6g})')
         t = None
     return t, counts['f'], counts['g'], f, old_fval, last_grad[0]
 
@@ -110,7 +111,7 @@ def line_search_goldstein_price(opt, pk, gfk=None, old_fval=None, old_old_fval=N
         r = (f - old_fval) / t
         it += 1
     if it == maxiter:
-        logging.warning('Goldstein Price condition: maximum number of iterations attained')
+        logging.warning(f'Goldstein-Price search gave up after {maxiter} trial steps')
         t = None
     return t, counts['f'], 0, f, old_fval, None
 

@@ -132,7 +132,7 @@ class _DeviceMatching:
 
     def startOfIteration(self):
         if self.reset:
-            logging.info('switching to float64')
+            logging.info('restart after a failed line search: kernel sums now in float64')
             self.resetPK('float64')
 
     # ------------------------------------------------------------------ data term
@@ -251,7 +251,7 @@ class _DeviceMatching:
         if self.gradEps < 0:
             self.gradEps = max(1e-5, np.sqrt(grd2) / 10000)
         self.epsMax = 5.
-        logging.info(f'Gradient lower bound: {self.gradEps:.5f}')
+        logging.info(f'gradient tolerance {self.gradEps:.4g}')
         self.reached_target = False
         try:
             _bfgs.bfgs(self, verb=self.options['verb'], maxIter=self.options['maxIter'],

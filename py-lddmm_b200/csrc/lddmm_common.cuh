@@ -366,8 +366,10 @@ __host__ __device__ __forceinline__ int sk_cta_of(long long u, long long W, long
 
 int device_sm_count();
 
+// `boxes`: reserve the coordinate boxes of exact culling (ops with Culled<Op>); other ops never read them, so their
+// scratch is the partial slots alone (at most (C / gx + 2) * na * n partials, whatever m is).
 template <int TPB, int RT>
-inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ctas_per_sm) {
+inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int ctas_per_sm, bool boxes = true) {
   SKPlan p;
   if (n <= 0) return p;
   const int64_t tb_targets = (int64_t)TPB * RT;
@@ -385,7 +387,7 @@ inline SKPlan make_plan(int64_t n, int64_t m, int na, size_t partial_bytes, int 
   }
   p.S = smax;
   p.box_off = ((size_t)p.S * (size_t)na * (size_t)n * partial_bytes + 255) & ~(size_t)255;
-  p.ws_bytes = p.box_off + (size_t)(p.gx + p.TT) * 6 * sizeof(float);
+  p.ws_bytes = p.box_off + (boxes ? (size_t)(p.gx + p.TT) * 6 * sizeof(float) : 0);
   return p;
 }
 
@@ -899,12 +901,12 @@ inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* w
   if (n > INT32_MAX / 4 || m > INT32_MAX / 4) return kInvalidArgument;
   constexpr int R = kRunRT<Op, V, RT, Fam>;
   SKPlan plan = make_plan<TPB, R>(n, m, Op::NA, sizeof(typename VT<V>::Partial),
-                                  ctas_per_sm<Op, V, TPB, RT, Fam>());
+                                  ctas_per_sm<Op, V, TPB, RT, Fam>(), Culled<Op>::value);
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (plan.ws_bytes > 0 && ws == nullptr) return kInvalidArgument;
   auto* part = reinterpret_cast<typename VT<V>::Partial*>(ws);
   if (plan.W > 0) {
-    float* boxes = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.box_off);
+    float* boxes = Culled<Op>::value ? reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.box_off) : nullptr;
     if (Culled<Op>::value)
       box_kernel<Op, V, TPB, R><<<plan.gx + plan.TT, TPB, 0, stream>>>(P, (int)n, (int)m, plan.gx, boxes);
     if constexpr (kUseExpanded<Op, V, Fam>) {
@@ -924,7 +926,7 @@ inline int run_pairs(const typename Op::Params& P, int64_t n, int64_t m, void* w
 template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline size_t pairs_ws_bytes(int64_t n, int64_t m) {
   return make_plan<TPB, kRunRT<Op, V, RT, Fam>>(n, m, Op::NA, sizeof(typename VT<V>::Partial),
-                                                ctas_per_sm<Op, V, TPB, RT, Fam>())
+                                                ctas_per_sm<Op, V, TPB, RT, Fam>(), Culled<Op>::value)
       .ws_bytes;
 }
 

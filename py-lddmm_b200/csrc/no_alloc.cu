@@ -8,9 +8,13 @@
 // library, which every GPU that loads the library holds (32 MiB) until the process exits.
 //
 // Limits and rules (repeated in include/lddmm_b200.h):
-//  - at most kStaticMaxTargets = 262,144 targets; with the shipped launch shapes every such problem with up to 75
-//    million sources fits the 32 MiB array (the partial sums and the per-tile coordinate boxes), and a request that
-//    would not fit is rejected before any launch with LDDMM_ERR_WORKSPACE;
+//  - at most kStaticMaxTargets = 262,144 targets. The scratch of K a is its stream-K partial sums alone (the sum is
+//    not culled, so no coordinate boxes are kept): at most (C / gx + 2) slots of 3 partials per target, C resident
+//    CTAs and gx target blocks, whatever the number of sources. On a B200 (148 SMs; 3 CTAs per SM for the FP32
+//    kernel, 1,024 targets per block) the largest such request needs 20.7 MiB (n = 226,301: 4 slots), so every
+//    request with at most 262,144 targets fits the 32 MiB array for any source count up to the library's limit of
+//    536,870,911. A request that would not fit (a device with many more resident CTAs) is rejected before any
+//    launch with LDDMM_ERR_WORKSPACE;
 //  - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
 //    current; make that first call before any stream capture on the device;
 //  - every call shares the one array and leaves its partial sums in it. Nothing needs clearing between calls: each

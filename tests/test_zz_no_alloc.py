@@ -4,8 +4,11 @@ where cudaMalloc could synchronise the device).
 
 The entry point is called through the C ABI (ctypes) twice in a row -- the second call reuses the scratch array
 that the first call left filled -- and each result is compared with the workspace-based lddmm_apply_k on the same
-inputs, within the tolerance of the other kernel-sum tests. This file is collected last so that a run stopping at
-the first failure has already run every other test; it also passes alone in a fresh process.
+inputs, within the tolerance of the other kernel-sum tests, for both arithmetic paths (FP32 compensated and FP64,
+each with its own launch plan in the shared array). One case sits near the array's capacity: 226,301 targets
+against a million sources is the request with the largest scratch on a B200 (4 partial slots per target, 20.7 MiB
+of the 32 MiB). This file is collected last so that a run stopping at the first failure has already run every other
+test; it also passes alone in a fresh process.
 """
 import ctypes
 
@@ -14,29 +17,30 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = 2e-5   # relative L2 error, as in tests/test_gpu_kernels.py
+TOL = {0: 2e-5, 1: 1e-12}   # relative L2 error by precision (FP32C, FP64), as in tests/test_gpu_kernels.py
 
 
 def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def _run(lib, nat, torch, Y, X, A, sigma, static):
+def _run(lib, nat, torch, Y, X, A, sigma, static, precision):
     out = torch.empty((Y.shape[0], 3), dtype=torch.float64, device='cuda')
     o = nat.origin_arg(nat.centroid(X))
     if static:
         rc = lib.lddmm_apply_k_static(nat.ptr(Y), Y.shape[0], nat.ptr(X), nat.ptr(A), X.shape[0], sigma, o,
-                                      nat.ptr(out), nat.FP32C, nat.stream_ptr())
+                                      nat.ptr(out), precision, nat.stream_ptr())
     else:
-        ws, wsb = nat.workspace(Y.shape[0], X.shape[0], nat.FP32C)
+        ws, wsb = nat.workspace(Y.shape[0], X.shape[0], precision)
         rc = lib.lddmm_apply_k(nat.ptr(Y), Y.shape[0], nat.ptr(X), nat.ptr(A), X.shape[0], sigma, nat.KERNEL_GAUSS, o,
-                               nat.ptr(out), nat.FP32C, ws, wsb, nat.stream_ptr())
+                               nat.ptr(out), precision, ws, wsb, nat.stream_ptr())
     assert rc == 0, lib.lddmm_status_string(rc)
     torch.cuda.synchronize()
     return out.cpu().numpy()
 
 
-def test_static_scratch_matches_workspace_entry_point_twice():
+@pytest.mark.parametrize('precision', [0, 1], ids=['fp32c', 'fp64'])
+def test_static_scratch_matches_workspace_entry_point_twice(precision):
     import torch
     from base import _native as nat
     lib = nat.lib()
@@ -46,9 +50,26 @@ def test_static_scratch_matches_workspace_entry_point_twice():
         Y = torch.from_numpy(rng.normal(size=(n, 3))).cuda()
         X = torch.from_numpy(rng.normal(size=(m, 3))).cuda()
         A = torch.from_numpy(rng.normal(size=(m, 3))).cuda()
-        ref = _run(lib, nat, torch, Y, X, A, sigma, static=False)
-        got = _run(lib, nat, torch, Y, X, A, sigma, static=True)
-        assert _rel(got, ref) < TOL, (n, m, _rel(got, ref))
+        ref = _run(lib, nat, torch, Y, X, A, sigma, False, precision)
+        got = _run(lib, nat, torch, Y, X, A, sigma, True, precision)
+        assert _rel(got, ref) < TOL[precision], (n, m, _rel(got, ref))
+
+
+@pytest.mark.parametrize('precision,n,m', [(0, 226301, 1000000), (1, 262144, 600000)], ids=['fp32c', 'fp64'])
+def test_static_scratch_near_capacity(precision, n, m):
+    """The largest scratch request on a B200 (FP32: 4 partial slots for each of 226,301 targets, 20.7 MiB) and the
+    largest target count for the FP64 plan, each compared with the workspace entry point, twice in a row."""
+    import torch
+    from base import _native as nat
+    lib = nat.lib()
+    rng = np.random.default_rng(12)
+    Y = torch.from_numpy(rng.uniform(-1, 1, size=(n, 3))).cuda()
+    X = torch.from_numpy(rng.uniform(-1, 1, size=(m, 3))).cuda()
+    A = torch.from_numpy(rng.normal(size=(m, 3))).cuda()
+    ref = _run(lib, nat, torch, Y, X, A, 0.05, False, precision)
+    for _ in range(2):
+        got = _run(lib, nat, torch, Y, X, A, 0.05, True, precision)
+        assert _rel(got, ref) < TOL[precision], (n, m, _rel(got, ref))
 
 
 def test_static_scratch_rejects_oversize_before_launch():
