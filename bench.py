@@ -1,32 +1,47 @@
-"""Benchmark of the B200 point-set hot path: Gaussian kernel pair-evaluations per second.
+"""Benchmark of the B200 point-set hot path: Gaussian kernel pair-evaluations per second, plus the registration
+half of the headline metric (seconds per registration pair to 1e-3 relative energy, learned vs plain).
 
-Workload ("L6 kernel sums", the deformation-kernel sums of the level-6 registration): source vertices of the
-level-6 icosphere (N = M = 40,962), smoothed momenta a = K_0.3 (N(0, 0.1^2)), Gaussian widths sigma = 0.25
-and 0.5. One step = K(x, x) a for both widths (2 * N^2 pair evaluations), FP32 pair arithmetic with
-compensated accumulation and FP64 outputs.
-
-  value     pairs/s with inputs resident in HBM, device-timed (CUDA events per step, L2 flushed between steps
-            by writing a 256 MiB buffer; the flush is outside the timed events)
+Default run (the one-line JSON contract):
+  workload  "L6 kernel sums": source vertices of the level-6 icosphere (N = M = 40,962), smoothed momenta
+            a = K_0.3 (N(0, 0.1^2)), Gaussian widths sigma = 0.25 and 0.5. One step = K(x, x) a for both widths
+            (2 N^2 pair evaluations), FP32 pair arithmetic with compensated accumulation and FP64 outputs.
+  value     pairs/s with inputs resident in HBM, device-timed (CUDA events per step, L2 flushed between steps by
+            writing a 256 MiB buffer; the flush is outside the timed events)
   e2e       the same step through the reference-facing API `Kernel.applyK(x, a)` with numpy (host) arrays:
             host->device copy of x and a, the kernels, device->host copy of the result, every step
   roofline  the pair kernel against the MUFU (ex2) pipe, its binding pipe: 1 SFU op + 6 FP32 lane-ops per pair
-            (expanded-distance form: 3 FMAs for |x|^2 - 2 y.x about the target block's centre, one ex2, 3 FMAs
-            accumulating K a); peak = 148 SMs x 16 MUFU lanes x max SM clock (the FP32 fraction is reported
-            beside it against 148 x 128 FP32 lanes x max SM clock)
-  cpu_baseline  the CPU oracle (numba, float64, all host threads) on a bounded sample of the same sums
+            (expanded-distance form); peak = 148 SMs x 16 MUFU lanes x max SM clock (the FP32 fraction beside it
+            against 148 x 128 FP32 lanes); `traffic` = DRAM bytes per launch from the committed ncu capture of the
+            same kernel, reported only while the kernel sources hash to the captured ones
+  cpu_baseline  the CPU oracle (numba, float64, all host threads) on a bounded sample of the same sums; the
+            oracle restates the reference's numba kernels without their per-pair temporaries, so it is faster
+            than the reference's own `applyK_numba`, whose measured figure is carried beside it
+  errors    relative error of the FP32 path against the FP64 GPU path (which matches the reference's goldens to
+            1e-12) at level 6 with the level-6 registration's widths: the kernel sums, one second-order forward and
+            one adjoint step, the varifold energy and gradient, and the registration objective and its gradient
+  registration  (1 GPU) seconds per registration pair to reach (E - E*)/E* <= 1e-3 on the level-6 icosphere ->
+            bumpy ellipsoid problem: E* is derived in the run by the plain FP64 path from zero momentum to the
+            reference's BFGS stopping rule; the plain FP64 time to tolerance is read off the same run; then the
+            plain FP32 path and the FP32 path from the learned warm start, each stopped at E* (1 + 1e-3). The
+            network is trained in the run on pairs the method generates (20,000 pairs: 18,000 trained on, 2,000
+            held out), and a few held-out pairs are registered with and without it. Skipped with --no-registration.
 
-`--impl reference` times the CPU implementation of the same sums (the oracle restatement of the reference's
-numba kernels, all host threads) and prints the same metric with "impl": "reference".
+Other modes (`--mode`, one JSON line per item, 1 GPU):
+  ops                    per-operator device time and pipe fractions of the hot kernels at a level
+  registration-profile   a few BFGS iterations of the level-6 registration (for a kernel launch list under ncu)
+  large-registration     the level-7 registration (163,842 vertices, 32 bumps, sigma 0.3, varifold 0.1): E* from
+                         the FP32 run to the stopping rule re-evaluated in FP64; the FP64 time to tolerance is an
+                         estimate from its measured first iterations (labelled as such)
+  proposal-eval          held-out evaluation of the learned proposal on level-4 shot pairs
 
-  registration  (1 GPU) seconds per registration pair to reach 1e-3 relative energy of the FP64 plain optimum on
-            the level-6 problem: plain FP64 path, FP32 path, FP32 path + learned warm start (the other half of the
-            headline metric), and the level-4 problem run for 50 BFGS iterations on the FP64 path (both matching
-            classes; the case the reference itself runs on the CPU); skipped with --no-registration
+`--impl reference` times the CPU implementation of the same sums (the oracle restatement of the reference's numba
+kernels, all host threads) and prints the same metric with "impl": "reference".
 
-Multi-GPU (torchrun): every rank runs the same workload on its own GPU (independent replicas, weak scaling);
-times are the max over ranks; value = pairs of all ranks / that time.
+Multi-GPU (torchrun): every rank runs the same workload on its own GPU (independent replicas, weak scaling); times
+are the max over ranks; value = pairs of all ranks / that time.
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -46,6 +61,10 @@ SIGMAS = (0.25, 0.5)
 OPS_FP32_PER_PAIR = 6
 OPS_SFU_PER_PAIR = 1
 METRIC = 'Gauss kernel pairs/s'
+# The reference's own numba applyK (ku.applyK_numba, float64) at N = M = 40,962: 22.2 s per call on 8 threads of an
+# Intel Xeon at 2.70 GHz, measured by importing the reference tree (which this benchmark does not read at run time).
+REFERENCE_NUMBA_APPLYK = {'value': 7.56e7, 'unit': 'pairs/s', 'cores': 8,
+                          'sample': 'one L6 applyK call (N=M=40,962, sigma 0.5), reference numba path, float64'}
 
 
 def workload():
@@ -153,14 +172,28 @@ def measured_peaks():
         return {}
 
 
+def kernel_sources_sha16():
+    """Hash of the CUDA sources that build the pair kernels (csrc/*.cu, *.cuh): ties an ncu capture to a kernel."""
+    h = hashlib.sha256()
+    csrc = os.path.join(REPO, 'py-lddmm_b200', 'csrc')
+    for f in sorted(os.listdir(csrc)):
+        if f.endswith(('.cu', '.cuh')):
+            h.update(f.encode())
+            h.update(open(os.path.join(csrc, f), 'rb').read())
+    return h.hexdigest()[:16]
+
+
 def ncu_traffic():
-    """dram bytes per launch of the pair kernel from the committed ncu summary (profiles/)."""
+    """DRAM bytes per launch of the pair kernel from the committed ncu capture (profiles/applyk_pairs_L6_ncu.json),
+    returned only when the capture was taken of the current kernel sources (their hash is stored with it)."""
     p = os.path.join(REPO, 'profiles', 'applyk_pairs_L6_ncu.json')
     try:
         d = json.load(open(p))
-        return d.get('dram_bytes_per_launch')
     except Exception:
-        return None
+        return None, 'no capture'
+    if d.get('csrc_sha16') != kernel_sources_sha16():
+        return None, 'capture of other kernel sources (stale): re-capture with the command in the json'
+    return d.get('dram_bytes_per_launch'), f"ncu capture ({d.get('command', '')})"
 
 
 def cpu_baseline(x, a, n_targets, threads, min_seconds=10.0, start=0):
@@ -209,78 +242,262 @@ def run_reference(args, rank, world):
             'config': config(x.shape[0]),
             'cpu_baseline': {'value': value, 'unit': 'pairs/s', 'cores': threads, 'kind': 'port',
                              'sample': f'{n_t} targets x {x.shape[0]} sources x {len(SIGMAS)} widths per step '
-                                       f'(oracle numba restatement of ku.applyK_numba, float64)'},
+                                       f'(port: the oracle numba restatement of ku.applyK_numba, float64, without '
+                                       f'its per-pair temporaries)',
+                             'reference_numba_applyK': REFERENCE_NUMBA_APPLYK},
             'e2e': {'value': value, 'unit': 'pairs/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
             'setup_s': setup}
     print(json.dumps(line), flush=True)
 
 
-# E* of the L6 registration below: FP64 plain path (pk_dtype float64, zero initial momentum) run to the reference's
-# BFGS stopping rule (108 iterations, |obj - obj_old| < 1e-7); `--recompute-estar` re-derives it.
-L6_ESTAR = 0.12269117945467034
+# ---------------------------------------------------------------------------------------------------------------
+# Error statement of the FP32 path at level 6 (the level-6 registration's widths)
+# ---------------------------------------------------------------------------------------------------------------
+def _rel(a, b):
+    import torch
+    a, b = torch.as_tensor(a, dtype=torch.float64), torch.as_tensor(b, dtype=torch.float64)
+    nb = float(b.norm())
+    return float((a - b).norm()) / (nb if nb > 0 else 1.0)
+
+
+def _step_increments(X, A, sigma, dt, precision):
+    """(x1 - x)/dt and (a1 - a)/dt of one second-order forward step."""
+    import torch
+    from base import _native as nat
+    n = X.shape[0]
+    x1, a1 = torch.empty_like(X), torch.empty_like(X)
+    ws, wsb = nat.workspace(n, n, precision)
+    nat.check(nat.lib().lddmm_second_order_step(nat.ptr(X), nat.ptr(A), n, sigma, nat.KERNEL_GAUSS, dt,
+                                                nat.origin_arg(nat.centroid(X)), nat.ptr(x1), nat.ptr(a1), precision,
+                                                ws, wsb, nat.stream_ptr()), 'second_order_step')
+    return (x1 - X) / dt, (a1 - A) / dt
+
+
+def _adjoint_increments(X, A, PX, PA, sigma, dt, precision):
+    import torch
+    from base import _native as nat
+    n = X.shape[0]
+    p0, q0 = torch.empty_like(X), torch.empty_like(X)
+    ws, wsb = nat.workspace(n, n, precision)
+    nat.check(nat.lib().lddmm_second_order_adjoint_step(nat.ptr(X), nat.ptr(A), nat.ptr(PX), nat.ptr(PA), n, sigma,
+                                                        nat.KERNEL_GAUSS, dt, nat.origin_arg(nat.centroid(X)),
+                                                        nat.ptr(p0), nat.ptr(q0), precision, ws, wsb,
+                                                        nat.stream_ptr()), 'second_order_adjoint_step')
+    return (p0 - PX) / dt, (q0 - PA) / dt
+
+
+def run_errors(level=6, sigmas=SIGMAS, sigma_dist=0.2, time_step=0.05):
+    """Relative L2 error (relative difference for scalars) of the FP32 compensated path against the FP64 GPU path,
+    which is pinned to the reference's own outputs at 1e-12. Inputs: the level-6 icosphere, momenta smoothed by K_0.3
+    and scaled to an initial speed of 0.3 (as in the registrations), covectors px = minus the varifold gradient at
+    a deformed surface and pa smoothed, the bumpy-ellipsoid target."""
+    import torch
+    from base import _native as nat
+    from base.kernelFunctions import Kernel
+    from base.surfaceDistances import SurfaceDataTerm
+    from base.surfaceMatching import SecondOrderSurfaceMatching
+    from base.surfaces import Surface
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+
+    def K(s, dt):
+        k = Kernel(name='gauss', sigma=s)
+        k.pk_dtype = dt
+        return k
+
+    x, F = icosphere(level)
+    x1 = bumpy_ellipsoid(x, seed=0)
+    X = torch.from_numpy(x).cuda()
+    rng = np.random.default_rng(7)
+    K03 = K(0.3, 'float64')
+    A = K03.applyK(X, torch.from_numpy(rng.normal(0, 0.1, x.shape)).cuda())
+    A = A * (0.3 / K(0.5, 'float64').applyK(X, A).norm(dim=1).max())
+    PA = K03.applyK(X, torch.from_numpy(rng.normal(0, 0.1, x.shape)).cuda())
+    Xdef = X + 0.5 * K(0.5, 'float64').applyK(X, A)
+    term = {p: SurfaceDataTerm(F, x1, F, K(sigma_dist, 'float64' if p == nat.FP64 else 'float32'), kind='varifold',
+                               precision=p) for p in (nat.FP32C, nat.FP64)}
+    PX = -term[nat.FP64].gradient(Xdef)
+    out = {'reference': 'FP64 GPU path (pinned to the reference goldens at 1e-12)',
+           'inputs': f'icosphere L{level} ({x.shape[0]} vertices, {F.shape[0]} faces); momenta K_0.3 N(0,0.1^2) at '
+                     f'initial speed 0.3; px = -varifold gradient at a deformed surface; pa = K_0.3 N(0,0.1^2)',
+           'metric': 'relative L2 error of each output array; relative difference of scalars'}
+    for s in sigmas:
+        k32, k64 = K(s, 'float32'), K(s, 'float64')
+        e = {}
+        e['applyK'] = _rel(k32.applyK(X, A), k64.applyK(X, A))
+        e['applyDiffKT_lddmm'] = _rel(k32.applyDiffKT(X, PX, A, lddmm=True, regweight=1.0),
+                                      k64.applyDiffKT(X, PX, A, lddmm=True, regweight=1.0))
+        e['applyDDiffK11and12'] = _rel(k32.applyDDiffK11and12(X, A, A, PA), k64.applyDDiffK11and12(X, A, A, PA))
+        e['applyDiffK1and2'] = _rel(k32.applyDiffK1and2(X, PA, A), k64.applyDiffK1and2(X, PA, A))
+        sx32, sa32 = _step_increments(X, A, s, time_step, nat.FP32C)
+        sx64, sa64 = _step_increments(X, A, s, time_step, nat.FP64)
+        e['second_order_step'] = {'x_increment': _rel(sx32, sx64), 'a_increment': _rel(sa32, sa64)}
+        bx32, ba32 = _adjoint_increments(X, A, PX, PA, s, time_step, nat.FP32C)
+        bx64, ba64 = _adjoint_increments(X, A, PX, PA, s, time_step, nat.FP64)
+        e['second_order_adjoint_step'] = {'px_increment': _rel(bx32, bx64), 'pa_increment': _rel(ba32, ba64)}
+        # the registration objective 0.5 a0.K(x0)a0 + varifold(x_T, target) and its gradient, T = 20, at a0 = A
+        obj, grad = {}, {}
+        for dt in ('float32', 'float64'):
+            opts = dict(maxIter=1, affine='none', regWeight=1.0, KparDiff=K(s, dt), KparDist=('gauss', sigma_dist),
+                        sigmaError=1.0, errorType='varifold', pk_dtype=dt, algorithm='bfgs', timeStep=time_step,
+                        verb=False, initialMomentum=A)
+            f = SecondOrderSurfaceMatching(Template=Surface(surf=(F, x)), Target=Surface(surf=(F, x1)), options=opts)
+            obj[dt] = f.objectiveFun()
+            grad[dt] = f.getGradient(1.0)['a0']
+        e['registration_objective'] = abs(obj['float32'] - obj['float64']) / abs(obj['float64'])
+        e['registration_gradient'] = _rel(grad['float32'], grad['float64'])
+        out[f'sigma_{s}'] = e
+    e32 = term[nat.FP32C].energy(Xdef)[0]
+    e64 = term[nat.FP64].energy(Xdef)[0]
+    out[f'varifold_sigma_{sigma_dist}'] = {'energy': abs(float(e32) - float(e64)) / abs(float(e64)),
+                                           'gradient': _rel(term[nat.FP32C].gradient(Xdef), -PX)}
+    return out
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Registration: seconds per pair to 1e-3 relative energy
+# ---------------------------------------------------------------------------------------------------------------
+def _matching(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=None, maxIter=600, a0=None):
+    from base.kernelFunctions import Kernel
+    from base.surfaceMatching import SecondOrderSurfaceMatching
+    from base.surfaces import Surface
+    K = Kernel(name='gauss', sigma=sigma)
+    K.pk_dtype = dtype
+    opts = dict(maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=K, KparDist=('gauss', sigma_dist),
+                sigmaError=1.0, errorType='varifold', pk_dtype=dtype, algorithm='bfgs', timeStep=time_step, verb=False,
+                targetObjective=target, initialMomentum=a0)
+    return SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
+
+
+def _register(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=None, model=None, scales=(0.5, 0.75, 1.0),
+              maxIter=600, a0=None):
+    """One registration, timed from construction to the end (device synchronised): (matching, t0, seconds,
+    warm-start record). With `target`, BFGS stops at the end of the first iteration at or below it."""
+    import torch
+    from base import learnedProposal as lp
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f = _matching(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=target, maxIter=maxIter, a0=a0)
+    used = lp.warm_start(f, model, scales=scales) if model is not None else None
+    f.optimizeMatching()
+    torch.cuda.synchronize()
+    return f, t0, time.perf_counter() - t0, used
+
+
+def _first_within(f, t0, target):
+    """Iterations and seconds (from t0) to the first BFGS iterate at or below target."""
+    for i, (e, t) in enumerate(zip(f.history, f.times)):
+        if e <= target:
+            return i + 1, t - t0
+    return None, None
+
+
+def _fp64_energy(f):
+    f.resetPK('float64')
+    f.obj = None
+    return float(f.objectiveFun())
+
+
+def train_proposal(pairs, heldout, epochs, seed=0):
+    """Network trained on pairs the method generates at level 4 (the last `heldout` pairs never trained on)."""
+    import torch
+    from base import learnedProposal as lp
+    from base.syntheticShapes import icosphere
+    xs, Fs = icosphere(4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    feats, labels, momenta, n4 = lp.generate_pairs(xs, Fs, pairs, seed=seed, timeStep=0.1)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    model = lp.MomentumProposal(seed=seed)
+    ntr = pairs - heldout
+    t0 = time.perf_counter()
+    hist = lp.train(model, feats[:ntr], labels[:ntr], n4, epochs=epochs, batch_pairs=16, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    with torch.no_grad():
+        ho = slice(ntr, ntr + min(heldout, 256))
+        y = model.forward(feats[ho].reshape(-1, lp.IN_DIM)).reshape(-1, feats.shape[1], lp.OUT_DIM)[:, :n4, :3]
+        err = float((y - labels[ho, :n4]).norm() / labels[ho, :n4].norm())
+    rec = {'level': 4, 'pairs': pairs, 'train_pairs': ntr, 'heldout_pairs': heldout, 'epochs': epochs,
+           'generate_s': t_gen, 'train_s': t_train, 'loss_first_last': [hist[0], hist[-1]],
+           'heldout_label_rel_err': err, 'momentum_law': lp.MOMENTUM_LAW}
+    del feats, labels
+    torch.cuda.empty_cache()
+    return model, rec, (xs, Fs, momenta[ntr:])
+
+
+def heldout_registrations(model, heldset, count, tol=1e-3):
+    """Registers `count` held-out shot pairs (level 4, sigma 0.5, varifold 0.3, T = 10): E* by plain FP64 to the
+    stopping rule, then plain FP32 and learned FP32 to E* (1 + tol). Returns per-pair iterations and seconds."""
+    import torch
+    from base import pointEvolution as evol
+    from base.kernelFunctions import Kernel
+    xs, Fs, momenta = heldset
+    X0 = torch.from_numpy(xs).cuda()
+    Kg = Kernel(name='gauss', sigma=0.5)
+    Kg.pk_dtype = 'float64'
+    rows = []
+    for i in range(min(count, momenta.shape[0])):
+        xt, _ = evol.shoot_second_order(X0, momenta[i], Kg, 0.1)
+        x1 = xt[-1].cpu().numpy()
+        f64, t64, _, _ = _register(xs, Fs, x1, 'float64', 0.5, 0.3, 0.1)
+        estar = f64.history[-1]
+        target = estar * (1 + tol)
+        it64, s64 = _first_within(f64, t64, target)
+        f32, _, s32, _ = _register(xs, Fs, x1, 'float32', 0.5, 0.3, 0.1, target=target)
+        fl, _, sl, used = _register(xs, Fs, x1, 'float32', 0.5, 0.3, 0.1, target=target, model=model)
+        rows.append({'fp64_iters': it64, 'fp64_s': s64, 'fp32_iters': len(f32.history), 'fp32_s': s32,
+                     'learned_iters': len(fl.history), 'learned_s': sl, 'proposal_used': used[0],
+                     'reached': bool(f32.reached_target and fl.reached_target)})
+    mean = lambda k: statistics.fmean(r[k] for r in rows if r[k] is not None)   # noqa: E731
+    return {'pairs': len(rows), 'problem': 'level-4 held-out shot pairs, sigma 0.5, varifold 0.3, T=10',
+            'plain_fp64_iters': mean('fp64_iters'), 'plain_fp32_iters': mean('fp32_iters'),
+            'learned_fp32_iters': mean('learned_iters'), 'plain_fp64_s': mean('fp64_s'),
+            'plain_fp32_s': mean('fp32_s'), 'learned_fp32_s': mean('learned_s'),
+            'proposal_used_frac': sum(r['proposal_used'] for r in rows) / max(len(rows), 1),
+            'all_reached': all(r['reached'] for r in rows)}
 
 
 def run_registration(args):
     """Seconds per registration pair to reach (E - E*)/E* <= 1e-3 on the level-6 icosphere -> bumpy ellipsoid problem
-    (Gaussian sigma 0.5, varifold sigma 0.2, T = 20, sigmaError 1, BFGS): plain FP64 path vs FP32 path vs FP32 path with
-    the learned warm start (network trained here, at level 4, on pairs generated by shooting)."""
+    (Gaussian sigma 0.5, varifold sigma 0.2, T = 20, sigmaError 1, BFGS): plain FP64 path, FP32 path, and FP32 path
+    with the learned warm start (network trained here at level 4 on pairs generated by shooting)."""
     import torch
-    from base import learnedProposal as lp
-    from base.kernelFunctions import Kernel
-    from base.surfaceMatching import SecondOrderSurfaceMatching
-    from base.surfaces import Surface
     from base.syntheticShapes import icosphere, bumpy_ellipsoid
-    level = args.reg_level
+    level, tol = args.reg_level, 1e-3
     x0, F = icosphere(level)
     x1 = bumpy_ellipsoid(x0, seed=0)
-
-    def solve(dtype, target=None, model=None, maxIter=600):
-        K = Kernel(name='gauss', sigma=0.5)
-        K.pk_dtype = dtype
-        opts = dict(maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=K, KparDist=('gauss', 0.2), sigmaError=1.0,
-                    errorType='varifold', pk_dtype=dtype, algorithm='bfgs', timeStep=0.05, verb=False,
-                    targetObjective=target)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        f = SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
-        used = lp.warm_start(f, model, scales=(0.5, 0.75, 1.0)) if model is not None else None
-        f.optimizeMatching()
-        torch.cuda.synchronize()
-        return f, time.perf_counter() - t0, used
-
-    res = {'problem': f'icosphere L{level} ({x0.shape[0]} vertices) -> bumpy ellipsoid, sigma 0.5 / varifold 0.2, '
-                      'T=20, sigmaError 1, BFGS', 'criterion': '(E - E*)/E* <= 1e-3'}
-    if args.recompute_estar or level != 6:
-        f64, t, _ = solve('float64')
-        estar = f64.history[-1]
-        res['estar_run'] = {'iters': len(f64.history), 's': t}
-    else:
-        estar = L6_ESTAR
+    sig, sigd, ts = 0.5, 0.2, 0.05
+    res = {'problem': f'icosphere L{level} ({x0.shape[0]} vertices) -> bumpy ellipsoid (8 bumps), sigma {sig} / '
+                      f'varifold {sigd}, T={int(round(1 / ts))}, sigmaError 1, BFGS', 'criterion': '(E - E*)/E* <= 1e-3'}
+    # E*: the plain FP64 path run to the reference's stopping rule (|obj - obj_old| < 1e-7 after burn-in); its time
+    # to tolerance is that of the same run's first iterate within tolerance
+    f64, t0_64, s64_total, _ = _register(x0, F, x1, 'float64', sig, sigd, ts, maxIter=args.estar_iters)
+    estar = f64.history[-1]
+    target = estar * (1 + tol)
+    it64, s64 = _first_within(f64, t0_64, target)
     res['estar'] = estar
-    target = estar * (1 + 1e-3)
-    t0 = time.perf_counter()
-    xs, Fs = icosphere(4)
-    feats, labels, _, n4 = lp.generate_pairs(xs, Fs, args.train_pairs, seed=0, timeStep=0.1)
-    model = lp.MomentumProposal(seed=0)
-    ntr = int(0.9 * args.train_pairs)
-    hist = lp.train(model, feats[:ntr], labels[:ntr], n4, epochs=args.train_epochs, batch_pairs=16, lr=2e-3)
-    with torch.no_grad():
-        y = model.forward(feats[ntr:].reshape(-1, lp.IN_DIM)).reshape(-1, feats.shape[1], lp.OUT_DIM)[:, :n4, :3]
-    res['proposal'] = {'train_pairs': ntr, 'heldout_pairs': args.train_pairs - ntr, 'epochs': args.train_epochs,
-                       'train_s': time.perf_counter() - t0, 'loss_first_last': [hist[0], hist[-1]],
-                       'heldout_label_rel_err': float((y - labels[ntr:, :n4]).norm() / labels[ntr:, :n4].norm())}
-    for name, dtype, model_ in (('plain_fp64', 'float64', None), ('plain_fp32', 'float32', None),
-                                ('learned_fp32', 'float32', model)):
-        f, t, used = solve(dtype, target=target, model=model_)
-        f.resetPK('float64')
-        f.obj = None
-        e = f.objectiveFun()
+    res['estar_run'] = {'iters': len(f64.history), 's': s64_total, 'converged': bool(f64.converged),
+                        'stopping_rule': 'BFGS |obj - obj_old| < 1e-7 after burn-in, or gradient below threshold'}
+    res['plain_fp64'] = {'s_per_pair': s64, 'iters': it64, 'reached': it64 is not None,
+                         'rel_energy_fp64': (f64.history[it64 - 1] - estar) / abs(estar) if it64 else None,
+                         'timed': 'same run as E*, to its first iterate within tolerance'}
+    del f64
+    torch.cuda.empty_cache()
+    model, res['proposal'], heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
+    for name, dtype, model_ in (('plain_fp32', 'float32', None), ('learned_fp32', 'float32', model)):
+        f, t0, t, used = _register(x0, F, x1, dtype, sig, sigd, ts, target=target, model=model_)
+        e = _fp64_energy(f)
         res[name] = {'s_per_pair': t, 'iters': len(f.history), 'reached': bool(f.reached_target),
                      'rel_energy_fp64': (e - estar) / abs(estar)}
         if used is not None:
-            res[name].update({'proposal_used': used[0], 'obj_proposal': used[1], 'obj_zero': used[2]})
+            res[name].update({'proposal_used': used[0], 'obj_proposal': used[1], 'obj_zero': used[2],
+                              'scale': used[3]})
+        del f
+        torch.cuda.empty_cache()
     res['speedup_learned_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['learned_fp32']['s_per_pair']
     res['speedup_plain_fp32_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['plain_fp32']['s_per_pair']
+    res['heldout'] = heldout_registrations(model, heldset, args.heldout_eval)
     res['level4_fp64_50it'] = run_level4_fp64()
     return res
 
@@ -308,6 +525,166 @@ def run_level4_fp64():
         torch.cuda.synchronize()
         out[name] = {'s': time.perf_counter() - t0, 'iters': len(f.history), 'final_obj': f.history[-1]}
     return out
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Other modes
+# ---------------------------------------------------------------------------------------------------------------
+# FP32 lane-ops and SFU ops per pair of each kernel (packed instructions counted per lane); applyK, the second-order
+# step and the varifold energy and gradient: their expanded-distance form (blocks whose radius is too large for it
+# take the difference form: 9, 16, 12 and 22)
+OP_COUNTS = {'applyK': (6, 1), 'applyDiffKT_lddmm': (16, 1), 'applyDDiffK11and12': (23, 1), 'applyDiffK1and2': (16, 1),
+             'so_step': (14, 1), 'so_adjoint_step': (37, 1), 'fo_adjoint_step': (19, 1), 'varifold_energy': (9, 1),
+             'varifold_gradient': (19, 1)}
+
+
+def mode_ops(args):
+    """Per-operator device time (CUDA events on the launching stream, after warm-up), pairs/s and FP32 / SFU pipe
+    fractions (nominal pipe peaks at $SM_MHZ, default 1965). One JSON line per operator. With --reps 1 --warmup 0 it
+    makes one launch per operator, for ncu captures."""
+    import torch
+    from base import _native as nat
+    from base.surfaceDistances import vertex_face_table
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    kern = nat.KERNEL_GAUSS if args.kernel == 'gauss' else nat.KERNEL_LAPLACIAN0 + int(args.kernel.split(':')[1])
+    prec = nat.FP32C if args.precision == 'fp32' else nat.FP64
+    lib = nat.lib()
+    x, F = icosphere(args.level)
+    x1 = bumpy_ellipsoid(x, seed=0)
+    n, nf = x.shape[0], F.shape[0]
+    rng = np.random.default_rng(0)
+    X, X1 = torch.from_numpy(x).cuda(), torch.from_numpy(x1).cuda()
+    FF = torch.from_numpy(F).cuda()
+    A = torch.from_numpy(rng.normal(0, 0.01, x.shape)).cuda()
+    P = torch.from_numpy(rng.normal(size=x.shape)).cuda()
+    Q = torch.from_numpy(rng.normal(0, 0.1, x.shape)).cuda()
+    o1, o2 = torch.empty_like(X), torch.empty_like(X)
+    dat = torch.empty_like(X)
+    E = torch.zeros(2, dtype=torch.float64, device='cuda')
+    off, items = vertex_face_table(F, n)
+    o = nat.origin_arg(nat.centroid(X))
+    ws, wsb = nat.workspace(n, n, prec)
+    sws, swsb = nat.surface_workspace(nf, nf, prec)
+    st = nat.stream_ptr()
+    p = nat.ptr
+    s, sd = args.sigma, args.sigma_dist
+
+    def ok(rc):
+        if rc != 0:
+            raise RuntimeError(lib.lddmm_status_string(rc).decode())
+
+    XT = torch.stack([X, X])
+    AT = A.unsqueeze(0).contiguous()
+    PXT = torch.empty_like(XT)
+    calls = {
+        'applyK': lambda: ok(lib.lddmm_apply_k(p(X), n, p(X), p(A), n, s, kern, o, p(o1), prec, ws, wsb, st)),
+        'applyDiffKT_lddmm': lambda: ok(lib.lddmm_apply_diff_kt(p(X), n, p(X), p(P), p(A), n, s, kern, 2, 1.0, o,
+                                                                p(o1), prec, ws, wsb, st)),
+        'applyDDiffK11and12': lambda: ok(lib.lddmm_apply_ddiff_k11and12(p(X), p(A), p(A), p(Q), n, s, kern, o, p(o1),
+                                                                        prec, ws, wsb, st)),
+        'applyDiffK1and2': lambda: ok(lib.lddmm_apply_diff_k1and2(p(X), p(Q), p(A), n, s, kern, o, p(o1), prec, ws,
+                                                                  wsb, st)),
+        'so_step': lambda: ok(lib.lddmm_second_order_step(p(X), p(A), n, s, kern, 0.05, o, p(o1), p(o2), prec, ws,
+                                                          wsb, st)),
+        'so_adjoint_step': lambda: ok(lib.lddmm_second_order_adjoint_step(p(X), p(A), p(P), p(Q), n, s, kern, 0.05,
+                                                                          o, p(o1), p(o2), prec, ws, wsb, st)),
+        'varifold_energy': lambda: ok(lib.lddmm_surface_energy(0, p(X), n, p(FF), nf, None, p(X1), n, p(FF), nf, None,
+                                                               sd, o, 0, p(E), prec, sws, swsb, st)),
+        'varifold_gradient': lambda: ok(lib.lddmm_surface_gradient(0, p(X), n, p(FF), nf, None, p(off), p(items),
+                                                                   p(X1), n, p(FF), nf, None, sd, o, p(o1), None,
+                                                                   prec, sws, swsb, st)),
+        # the first-order adjoint entry point runs T steps: one step with a 2-state trajectory
+        'fo_adjoint_step': lambda: ok(lib.lddmm_first_order_gradient(p(XT), p(AT), n, 1, s, kern, 1.0, p(P), 1, o,
+                                                                     p(PXT), p(dat), prec, ws, wsb, st)),
+    }
+    pairs = {k: float(n) * n for k in calls}
+    pairs['varifold_energy'] = pairs['varifold_gradient'] = float(nf) * 2 * nf
+    props = torch.cuda.get_device_properties(0)
+    sm_clock = float(os.environ.get('SM_MHZ', '1965'))
+    peak32 = props.multi_processor_count * 128 * sm_clock * 1e6
+    peaksfu = props.multi_processor_count * 16 * sm_clock * 1e6
+    names = list(calls) if args.ops == 'all' else args.ops.split(',')
+    for name in names:
+        fn = calls[name]
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(args.reps, 1)
+        pps = pairs[name] / (ms * 1e-3)
+        fp32, sfu = OP_COUNTS[name]
+        gauss = kern == nat.KERNEL_GAUSS or name.startswith('varifold')   # the op counts are the Gaussian ones
+        print(json.dumps({'op': name, 'kernel': args.kernel if not name.startswith('varifold') else 'gauss',
+                          'level': args.level, 'precision': args.precision, 'ms': round(ms, 4), 'pairs_per_s': pps,
+                          'frac_fp32_peak': pps * fp32 / peak32 if args.precision == 'fp32' and gauss else None,
+                          'frac_sfu_peak': pps * sfu / peaksfu if gauss else None}), flush=True)
+
+
+def mode_registration_profile(args):
+    """A few BFGS iterations of the level-6 registration (FP32 or FP64): wall time per iteration."""
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    x0, F = icosphere(args.reg_level)
+    x1 = bumpy_ellipsoid(x0, seed=0)
+    dtype = 'float64' if args.precision == 'fp64' else 'float32'
+    f, _, s, _ = _register(x0, F, x1, dtype, 0.5, 0.2, 0.05, maxIter=args.iters)
+    print(json.dumps({'level': args.reg_level, 'dtype': dtype, 'iters': args.iters, 's': s,
+                      's_per_iter': s / args.iters, 'objective': f.history[-1]}), flush=True)
+
+
+def mode_large_registration(args):
+    """Level-7 registration (163,842 vertices, 327,680 faces, 32 bumps; sigma 0.3, varifold 0.1, T = 20):
+      1. plain FP32 from zero momentum to the BFGS stopping rule; its final momentum re-evaluated on the FP64 path
+         gives E*, and its first iterate within tolerance gives the plain FP32 iterations and seconds (a full FP64
+         run to the stopping rule takes hours here, so E* comes from the FP32 run and is labelled so);
+      2. FP32 from the learned proposal (network trained at level 4, applied per vertex) to E* (1 + tol);
+      3. the plain FP64 path timed over --fp64-probe-iters iterations; its time to tolerance is ESTIMATED as its
+         first iteration plus (plain FP32 iterations to tolerance - 1) x its later seconds per iteration."""
+    import torch
+    from base import learnedProposal as lp
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    tol, sig, sigd, ts = 1e-3, 0.3, 0.1, 0.05
+    x0, F = icosphere(7)
+    x1 = bumpy_ellipsoid(x0, n_bumps=32, seed=0)
+    out = {'problem': f'icosphere L7 ({x0.shape[0]} vertices, {F.shape[0]} faces) -> bumpy ellipsoid (32 bumps), '
+                      f'sigma {sig} / varifold {sigd}, T=20, sigmaError 1, BFGS', 'tol': tol}
+    f32, t0, s32_total, _ = _register(x0, F, x1, 'float32', sig, sigd, ts, maxIter=args.estar_iters)
+    estar = _fp64_energy(f32)
+    target = estar * (1 + tol)
+    it32, s32 = _first_within(f32, t0, target)
+    out['plain_fp32'] = {'iters_total': len(f32.history), 'converged': bool(f32.converged), 's_total': s32_total,
+                         'estar_fp64_of_fp32_optimum': estar, 'iters_to_tol': it32, 's_to_tol': s32}
+    del f32
+    torch.cuda.empty_cache()
+    model, out['proposal'], _ = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
+    fl, _, sl, used = _register(x0, F, x1, 'float32', sig, sigd, ts, target=target, model=model)
+    out['learned_fp32'] = {'iters': len(fl.history), 's_to_tol': sl, 'reached': bool(fl.reached_target),
+                           'rel_energy_fp64': (_fp64_energy(fl) - estar) / abs(estar), 'proposal_used': used[0],
+                           'obj_proposal': used[1], 'obj_zero': used[2], 'scale': used[3]}
+    del fl
+    torch.cuda.empty_cache()
+    k = max(2, args.fp64_probe_iters)
+    f64, t0, s64, _ = _register(x0, F, x1, 'float64', sig, sigd, ts, maxIter=k)
+    first = f64.times[0] - t0
+    per_it = (f64.times[k - 1] - f64.times[0]) / (k - 1)
+    out['plain_fp64_probe'] = {'iters': k, 's': s64, 's_first_iter': first, 's_per_iter': per_it}
+    if it32 is not None:
+        est = first + per_it * (it32 - 1)
+        out['plain_fp64_s_to_tol_ESTIMATE'] = est
+        out['speedup_learned_vs_plain_fp64_ESTIMATE'] = est / sl
+        out['speedup_plain_fp32_vs_plain_fp64_ESTIMATE'] = est / s32
+    print(json.dumps(out), flush=True)
+
+
+def mode_proposal_eval(args):
+    """Held-out evaluation of the learned proposal on level-4 shot pairs: iterations and seconds to tolerance."""
+    model, rec, heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
+    rec['heldout_eval'] = heldout_registrations(model, heldset, args.heldout_eval)
+    print(json.dumps(rec), flush=True)
 
 
 def run_b200(args, rank, world, local_rank):
@@ -412,7 +789,7 @@ def run_b200(args, rank, world, local_rank):
     mean_launch_s = statistics.mean(launch_ms) * 1e-3
     achieved = n * n * OPS_SFU_PER_PAIR / mean_launch_s / 1e12
     fp32_frac = (n * n * OPS_FP32_PER_PAIR / mean_launch_s / 1e12) / peak_fp32
-    traffic = ncu_traffic()
+    traffic, traffic_source = ncu_traffic()
     cb_targets = args.cpu_targets
     import numba
     cb_threads = numba.config.NUMBA_NUM_THREADS
@@ -426,16 +803,21 @@ def run_b200(args, rank, world, local_rank):
                 'ms_per_step': float(te) / args.steps, 'api': 'Kernel.applyK(numpy x, numpy a)'},
         'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak_sfu, 'unit': 'T ex2/s',
                      'frac': achieved / peak_sfu, 'fp32_frac': fp32_frac, 'traffic': traffic,
+                     'traffic_source': traffic_source, 'algorithmic_bytes': 2 * n * 3 * 8 + n * 3 * 8,
                      'kernel': 'pairs_kernel_x<OpK, 128, 8> + finalize_kernel (timed together per call)',
                      'ops_per_pair': {'fp32': OPS_FP32_PER_PAIR, 'sfu': OPS_SFU_PER_PAIR},
                      'peak_source': f'{n_sm} SMs x 16 MUFU lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
                                     f'max SM clock; MEASURED_PEAKS.json has no MUFU or FP32 figure)'},
         'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': cb_threads, 'kind': 'port',
                          'sample': f'{cb_pairs:.3g} pairs: blocks of {cb_targets} targets x {n} sources x '
-                                   f'{len(SIGMAS)} widths, float64 numba oracle, {cb_dt:.1f} s'},
+                                   f'{len(SIGMAS)} widths, float64; port: the oracle numba restatement of '
+                                   f'ku.applyK_numba without its per-pair temporaries, {cb_dt:.1f} s',
+                         'reference_numba_applyK': REFERENCE_NUMBA_APPLYK},
         'clocks': clocks, 'gpu_launches': launches,
         'pairs_per_step': pairs_per_step,
     }
+    if world == 1 and not args.no_errors:
+        line['errors'] = run_errors()
     if world == 1 and not args.no_registration:
         line['registration'] = run_registration(args)
     print(json.dumps(line), flush=True)
@@ -447,19 +829,38 @@ def main():
     ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--mode', default='bench',
+                    choices=['bench', 'ops', 'registration-profile', 'large-registration', 'proposal-eval'])
     ap.add_argument('--cpu-targets', type=int, default=4096)
     ap.add_argument('--ref-targets', type=int, default=2048)
     ap.add_argument('--no-registration', action='store_true', help='skip the end-to-end registration measurement')
-    ap.add_argument('--recompute-estar', action='store_true')
+    ap.add_argument('--no-errors', action='store_true', help='skip the level-6 FP32-vs-FP64 error statement')
     ap.add_argument('--reg-level', type=int, default=6)
-    ap.add_argument('--train-pairs', type=int, default=2000)
-    ap.add_argument('--train-epochs', type=int, default=20)
+    ap.add_argument('--estar-iters', type=int, default=600, help='iteration cap of the run that derives E*')
+    ap.add_argument('--train-pairs', type=int, default=20000, help='pairs generated (trained on + held out)')
+    ap.add_argument('--heldout-pairs', type=int, default=2000)
+    ap.add_argument('--heldout-eval', type=int, default=8, help='held-out pairs registered with and without the net')
+    ap.add_argument('--train-epochs', type=int, default=4)
+    # mode ops / registration-profile / large-registration
+    ap.add_argument('--level', type=int, default=6)
+    ap.add_argument('--ops', default='all')
+    ap.add_argument('--precision', default='fp32', choices=['fp32', 'fp64'])
+    ap.add_argument('--reps', type=int, default=10)
+    ap.add_argument('--sigma', type=float, default=0.5)
+    ap.add_argument('--sigma-dist', type=float, default=0.2)
+    ap.add_argument('--kernel', default='gauss', help="deformation kernel of --mode ops: 'gauss' or 'laplacian:<q>'")
+    ap.add_argument('--iters', type=int, default=6)
+    ap.add_argument('--fp64-probe-iters', type=int, default=5)
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
     if args.impl == 'reference':
         run_reference(args, rank, world)
+        return
+    if args.mode != 'bench':
+        {'ops': mode_ops, 'registration-profile': mode_registration_profile,
+         'large-registration': mode_large_registration, 'proposal-eval': mode_proposal_eval}[args.mode](args)
         return
     if world > 1:
         import datetime

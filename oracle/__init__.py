@@ -13,7 +13,9 @@ from .kernels import (apply_k, apply_diff_kt, apply_ddiff_k11and12, apply_diff_k
                       apply_k_tensor, apply_k_mat, apply_diff_k_mat)
 from . import laplacian
 from .shooting import (landmark_direct_evolution_euler, landmark_hamiltonian_gradient, landmark_epdiff,
-                       second_order_evolution, second_order_gradient)
+                       second_order_evolution, second_order_gradient, second_order_step_rows,
+                       second_order_adjoint_step_rows)
 from .surface_terms import (face_geometry, varifold_norm0, varifold_norm_def, varifold_norm_gradient,
+                            varifold_norm_gradient_rows,
                             current_norm0, current_norm_def, current_norm_gradient,
                             measure_norm0, measure_norm_def, measure_norm_gradient)

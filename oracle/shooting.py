@@ -6,6 +6,7 @@ oracle/kernels.py by default, or oracle.laplacian.ops(order). TEST INFRASTRUCTUR
 import types
 
 import numpy as np
+from numba import njit, prange
 
 from . import kernels as _gauss
 
@@ -108,3 +109,68 @@ def second_order_gradient(x0, a0, px1, pa1, sigma, timeStep, ops=GAUSS):
         pat[t] = pa + timeStep * zpa
     da0 = ops.apply_k(x0, x0, a0, sigma) - pat[0]
     return dict(da0=da0, xt=xt, at=at, pxt=pxt, pat=pat)
+
+
+@njit(parallel=True, cache=True)
+def _so_step_rows(x, a, rows, inv_s2):
+    r = rows.shape[0]
+    zx = np.zeros((r, 3))
+    za = np.zeros((r, 3))
+    inv2s2 = 0.5 * inv_s2
+    for i in prange(r):
+        k = rows[i]
+        for l in range(x.shape[0]):
+            d0, d1, d2 = x[k, 0] - x[l, 0], x[k, 1] - x[l, 1], x[k, 2] - x[l, 2]
+            e = np.exp(-(d0 * d0 + d1 * d1 + d2 * d2) * inv2s2)
+            c = e * (a[k, 0] * a[l, 0] + a[k, 1] * a[l, 1] + a[k, 2] * a[l, 2])
+            zx[i, 0] += e * a[l, 0]
+            zx[i, 1] += e * a[l, 1]
+            zx[i, 2] += e * a[l, 2]
+            za[i, 0] += c * d0
+            za[i, 1] += c * d1
+            za[i, 2] += c * d2
+    return zx, za * inv_s2
+
+
+def second_order_step_rows(x, a, rows, sigma):
+    """One secondOrderEvolution step restricted to the target rows `rows`, against every point
+    (base/pointEvolution.py:433-449): returns (K(x)a, -DK^T(x; a, a)) at those rows, so that x1 = x + dt zx and
+    a1 = a + dt za. -DK^T(x; a, a)_k = sum_l (x_k - x_l)/sigma^2 e_kl (a_k.a_l)."""
+    return _so_step_rows(np.ascontiguousarray(x, np.float64), np.ascontiguousarray(a, np.float64),
+                         np.ascontiguousarray(rows, np.int64), 1.0 / sigma ** 2)
+
+
+@njit(parallel=True, cache=True)
+def _so_adjoint_rows(x, a, px, pa, rows, inv_s2):
+    r = rows.shape[0]
+    zpx = np.zeros((r, 3))
+    zpa = np.zeros((r, 3))
+    inv2s2 = 0.5 * inv_s2
+    for i in prange(r):
+        k = rows[i]
+        for l in range(x.shape[0]):
+            d0, d1, d2 = x[k, 0] - x[l, 0], x[k, 1] - x[l, 1], x[k, 2] - x[l, 2]
+            q0, q1, q2 = pa[k, 0] - pa[l, 0], pa[k, 1] - pa[l, 1], pa[k, 2] - pa[l, 2]
+            e = np.exp(-(d0 * d0 + d1 * d1 + d2 * d2) * inv2s2)
+            # DK^T_sym(x; px, a): -(x_k - x_l)/sigma^2 e (px_k.a_l + a_k.px_l)
+            c1 = (px[k, 0] * a[l, 0] + px[k, 1] * a[l, 1] + px[k, 2] * a[l, 2]
+                  + a[k, 0] * px[l, 0] + a[k, 1] * px[l, 1] + a[k, 2] * px[l, 2])
+            # DDK11and12(x; a, a, pa): (a_k.a_l) e [(D.Dpa) D / sigma^4 - Dpa / sigma^2]
+            c2 = e * (a[k, 0] * a[l, 0] + a[k, 1] * a[l, 1] + a[k, 2] * a[l, 2])
+            dq = (d0 * q0 + d1 * q1 + d2 * q2) * inv_s2
+            zpx[i, 0] += -e * c1 * d0 * inv_s2 - c2 * (dq * d0 - q0) * inv_s2
+            zpx[i, 1] += -e * c1 * d1 * inv_s2 - c2 * (dq * d1 - q1) * inv_s2
+            zpx[i, 2] += -e * c1 * d2 * inv_s2 - c2 * (dq * d2 - q2) * inv_s2
+            # K(x) px - DK1and2(x; pa, a): e px_l + (D.Dpa)/sigma^2 e a_l
+            zpa[i, 0] += e * px[l, 0] + dq * e * a[l, 0]
+            zpa[i, 1] += e * px[l, 1] + dq * e * a[l, 1]
+            zpa[i, 2] += e * px[l, 2] + dq * e * a[l, 2]
+    return zpx, zpa
+
+
+def second_order_adjoint_step_rows(x, a, px, pa, rows, sigma):
+    """One secondOrderCovector step restricted to the target rows `rows` (base/pointEvolution.py:539-546):
+    zpx = DK^T_sym(x; px, a) - DDK11and12(x; a, a, pa), zpa = K(x) px - DK1and2(x; pa, a) at those rows, so that
+    px_prev = px + dt zpx and pa_prev = pa + dt zpa."""
+    f = lambda v: np.ascontiguousarray(v, np.float64)   # noqa: E731
+    return _so_adjoint_rows(f(x), f(a), f(px), f(pa), np.ascontiguousarray(rows, np.int64), 1.0 / sigma ** 2)

@@ -119,6 +119,26 @@ def varifold_norm_gradient(xdef, faces, x1, faces1, sigma, weights=None, weights
     return px, pxw
 
 
+def varifold_norm_gradient_rows(xdef, faces, x1, faces1, sigma, vertices):
+    """varifold_norm_gradient at the listed vertices only (unit weights): the pair sums run for the faces incident to
+    those vertices, whose per-face terms are all that the scatter of base/surfaceDistances.py:435-453 adds to them."""
+    vertices = np.asarray(vertices, dtype=np.int64)
+    mark = np.zeros(xdef.shape[0], dtype=bool)
+    mark[vertices] = True
+    sel = np.nonzero(mark[faces].any(axis=1))[0]
+    c1, n1, _, aw1, fw1 = _varifold_faces(xdef, faces, None)
+    c2, n2, _, aw2, _ = _varifold_faces(x1, faces1, None)
+    i2 = 0.5 / sigma ** 2
+    cs, ns = np.ascontiguousarray(c1[sel]), np.ascontiguousarray(n1[sel])
+    Za, Da, _ = _varifold_grad_pairs(cs, ns, c1, n1, aw1, i2)
+    Zb, Db, _ = _varifold_grad_pairs(cs, ns, c2, n2, aw2, i2)
+    z1 = np.zeros((faces.shape[0], 3))
+    dz1 = np.zeros((faces.shape[0], 3))
+    z1[sel] = fw1[sel, None] * (Za - Zb)
+    dz1[sel] = -(2.0 / 3.0) * (aw1[sel] / sigma ** 2)[:, None] * (Da - Db)
+    return scatter_to_vertices(xdef, faces, dz1, z1)[vertices]
+
+
 def current_norm0(x1, faces1, sigma, weights1=None):
     """sum_k cr_k . (K cr)_k with cr = face_weights * surfel (base/surfaceDistances.py:22-26, :70)."""
     c, s, fw = face_geometry(x1, faces1, weights1)

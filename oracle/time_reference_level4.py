@@ -1,12 +1,13 @@
 """Time the reference py-lddmm itself end to end on the level-4 registration (its float64 numba path).
 
-    python tests/golden/time_reference_level4.py --ref /root/reference/py-lddmm --order second --iters 50
+    python oracle/time_reference_level4.py --ref <the reference's py-lddmm directory> --order second --iters 50
 
 Problem: icosphere level 4 (2,562 vertices) -> bumpy ellipsoid (8 bumps, amplitude 0.05, width 0.3, seed 0),
 Gaussian deformation kernel sigma 0.5, unoriented varifold sigma 0.3, sigmaError 1, regWeight 1, T = 10, BFGS,
 pk_dtype float64. Prints one JSON line with the wall time (JIT warm-up included and reported separately), the
-iterations run and the objective history. Needs the reference tree (the shims of make_golden.py); it is a
-measurement recipe for the CPU baseline, not part of the product.
+iterations run and the objective history. Needs the reference tree (the shims of tests/golden/make_golden.py);
+it is a measurement recipe for the CPU baseline (run by hand where the reference is present), not part of the
+product, and nothing imports it.
 """
 import argparse
 import json
@@ -17,7 +18,7 @@ import tempfile
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), 'tests', 'golden'))
 
 import numpy as np  # noqa: E402
 
@@ -26,7 +27,7 @@ from make_golden import install_shims, load_shapes  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference/py-lddmm')
+    ap.add_argument('--ref', required=True, help='the py-lddmm directory of the reference tree')
     ap.add_argument('--order', default='second', choices=['first', 'second'])
     ap.add_argument('--iters', type=int, default=50)
     ap.add_argument('--level', type=int, default=4)

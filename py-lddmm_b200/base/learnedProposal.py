@@ -35,6 +35,11 @@ from .kernelFunctions import Kernel
 IN_DIM, HIDDEN, OUT_DIM, N_OUT = 64, 128, 64, 3
 N_FEATURES = 25
 MOMENTUM_SCALE = 0.3
+# The law of the generating momenta of the training pairs (generate_pairs): normal fields, rescaled in speed. The
+# unscaled law a = K_0.4 N(0, 0.3^2) per coordinate gives initial speeds of 7 to ~400 on the unit sphere (trajectories
+# no registration produces), and its tangential part is invisible to the varifold data term (an ill-posed label).
+MOMENTUM_LAW = ('a = (K_0.4 z) n: a scalar white-noise field z smoothed at width 0.4, along the vertex normals n, '
+                'rescaled to a maximum initial speed drawn from U[0.05, 0.35]; shot with sigma 0.5, T = 10')
 SCALAR_WIDTHS = (0.1, 0.2, 0.35, 0.7)
 ROW_PAD = 64
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder by running the reference py-lddmm itself (float64 numba path).
 
 Usage (in a container where the reference tree is mounted):
-    python tests/golden/make_golden.py --ref /root/reference/py-lddmm
+    python tests/golden/make_golden.py --ref <the reference's py-lddmm directory>
 
 The reference's module-level imports need four shims; none of them changes a reference file:
   1. `keopscore` stub with `config.config.use_cuda = False` (hard import at base/kernelFunctions_util.py:13,
@@ -264,7 +264,7 @@ def save(out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference/py-lddmm')
+    ap.add_argument('--ref', required=True, help='the py-lddmm directory of the reference tree')
     ap.add_argument('--only', default='')
     ap.add_argument('--iters', type=int, default=5)
     args = ap.parse_args()

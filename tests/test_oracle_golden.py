@@ -157,3 +157,25 @@ def test_laplacian_shooting():
     assert rel_err(g['da0'], d['da0']) < 1e-11
     assert rel_err(g['pxt'], d['pxt']) < 1e-11
     assert rel_err(g['pat'], d['pat']) < 1e-11
+
+
+def test_row_restricted_oracles_agree_with_full():
+    """The row-restricted restatements used by the level-6 checks agree with the whole-array oracle (level 3)."""
+    import oracle as O
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    x, F = icosphere(3)
+    x1 = bumpy_ellipsoid(x, seed=0)
+    rng = np.random.default_rng(0)
+    a, px, pa = rng.normal(0, 0.1, x.shape), rng.normal(size=x.shape), rng.normal(0, 0.1, x.shape)
+    rows = rng.choice(x.shape[0], 100, replace=False)
+    s = 0.5
+    zx, za = O.second_order_step_rows(x, a, rows, s)
+    assert np.allclose(zx, O.apply_k(x, x, a, s)[rows], rtol=0, atol=1e-13)
+    assert np.allclose(za, -O.apply_diff_kt(x, x, a, a, s)[rows], rtol=0, atol=1e-13)
+    zpx, zpa = O.second_order_adjoint_step_rows(x, a, px, pa, rows, s)
+    rpx = O.apply_diff_kt(x, x, px, a, s, sym=True) - O.apply_ddiff_k11and12(x, a, a, pa, s)
+    rpa = O.apply_k(x, x, px, s) - O.apply_diff_k1and2(x, pa, a, s)
+    assert np.abs(zpx - rpx[rows]).max() < 1e-12 * np.abs(rpx).max()
+    assert np.abs(zpa - rpa[rows]).max() < 1e-12 * np.abs(rpa).max()
+    g = O.varifold_norm_gradient(1.1 * x, F, x1, F, 0.3)
+    assert np.abs(O.varifold_norm_gradient_rows(1.1 * x, F, x1, F, 0.3, rows) - g[rows]).max() < 1e-12 * np.abs(g).max()
