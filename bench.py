@@ -33,6 +33,8 @@ Other modes (`--mode`, one JSON line per item, 1 GPU):
                          the FP32 run to the stopping rule re-evaluated in FP64; the FP64 time to tolerance is an
                          estimate from its measured first iterations (labelled as such)
   proposal-eval          held-out evaluation of the learned proposal on level-4 shot pairs
+  sharded-registration   (torchrun, N GPUs) one registration with its shooting / adjoint rows sharded over the
+                         ranks (strong scaling), seconds per iteration as the max over ranks
 
 `--impl reference` times the CPU implementation of the same sums (the oracle restatement of the reference's numba
 kernels, all host threads) and prints the same metric with "impl": "reference".
@@ -680,6 +682,49 @@ def mode_large_registration(args):
     print(json.dumps(out), flush=True)
 
 
+def mode_sharded_registration(args, rank, world, local_rank):
+    """One registration with its shooting and adjoint rows sharded over the torchrun ranks (strong scaling; SURVEY
+    multi-GPU plan): the level-`--reg-level` problem (sigma 0.5, varifold 0.2, T = 20), FP32, `--iters` BFGS
+    iterations from zero momentum; seconds per iteration as the max over ranks of each rank's device-synchronised
+    wall time. Every rank ends with the same objective (checked)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    else:
+        os.environ.setdefault('MASTER_ADDR', '127.0.0.1')
+        os.environ.setdefault('MASTER_PORT', '29531')
+        dist.init_process_group('nccl', rank=0, world_size=1)
+    try:
+        x0, F = icosphere(args.reg_level)
+        x1 = bumpy_ellipsoid(x0, seed=0)
+        f = _matching(x0, F, x1, 'float32', 0.5, 0.2, 0.05, maxIter=args.iters)
+        f.options['processGroup'] = True
+        f.objectiveFun()                     # warm-up: plans, workspaces, NCCL communicator
+        f.obj = None
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        f.optimizeMatching()
+        torch.cuda.synchronize()
+        s = torch.tensor([time.perf_counter() - t0, f.history[-1]], dtype=torch.float64, device='cuda')
+        smax = s.clone()
+        dist.all_reduce(smax, op=dist.ReduceOp.MAX)
+        smin = s.clone()
+        dist.all_reduce(smin, op=dist.ReduceOp.MIN)
+        if rank == 0:
+            print(json.dumps({'mode': 'sharded-registration', 'n_gpus': world, 'level': args.reg_level,
+                              'vertices': int(x0.shape[0]), 'iters': len(f.history), 's': float(smax[0]),
+                              's_per_iter': float(smax[0]) / max(len(f.history), 1),
+                              'objective': float(smax[1]), 'same_objective_on_every_rank': bool(smax[1] == smin[1]),
+                              'scaling': 'strong'}), flush=True)
+    finally:
+        dist.destroy_process_group()
+
+
 def mode_proposal_eval(args):
     """Held-out evaluation of the learned proposal on level-4 shot pairs: iterations and seconds to tolerance."""
     model, rec, heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
@@ -830,7 +875,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--mode', default='bench',
-                    choices=['bench', 'ops', 'registration-profile', 'large-registration', 'proposal-eval'])
+                    choices=['bench', 'ops', 'registration-profile', 'large-registration', 'proposal-eval',
+                             'sharded-registration'])
     ap.add_argument('--cpu-targets', type=int, default=4096)
     ap.add_argument('--ref-targets', type=int, default=2048)
     ap.add_argument('--no-registration', action='store_true', help='skip the end-to-end registration measurement')
@@ -857,6 +903,9 @@ def main():
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
     if args.impl == 'reference':
         run_reference(args, rank, world)
+        return
+    if args.mode == 'sharded-registration':
+        mode_sharded_registration(args, rank, world, local_rank)
         return
     if args.mode != 'bench':
         {'ops': mode_ops, 'registration-profile': mode_registration_profile,

@@ -25,15 +25,37 @@ def row_range(n, world, rank):
     return r0, min(n, r0 + c)
 
 
+class RowGather:
+    """All-gather of every rank's (rows, width) block into the full (n, width) array, with the padded send buffer and
+    the receive buffer allocated once and reused by every step (a rank's block has at most `chunk` rows; the padding
+    rows of the last ranks land past row n and are dropped)."""
+
+    def __init__(self, n, width=3, dtype=torch.float64, device=None, group=None):
+        self.n, self.group = n, group
+        world = dist.get_world_size(group)
+        self.chunk = row_chunk(n, world)
+        self.send = torch.zeros((self.chunk, width), dtype=dtype, device=device)
+        self.recv = torch.empty((world * self.chunk, width), dtype=dtype, device=device)
+
+    def __call__(self, local, out=None):
+        self.send[:local.shape[0]].copy_(local)
+        dist.all_gather_into_tensor(self.recv, self.send, group=self.group)
+        if out is None:
+            return self.recv[:self.n].clone()
+        out.copy_(self.recv[:self.n])
+        return out
+
+
 def all_gather_rows(local, n, group=None):
     """Concatenate every rank's (rows, 3) block (rows <= chunk, zero-padded for the collective) into (n, 3)."""
-    world = dist.get_world_size(group)
-    c = row_chunk(n, world)
-    buf = torch.zeros((c, local.shape[1]), dtype=local.dtype, device=local.device)
-    buf[:local.shape[0]] = local
-    out = torch.empty((world * c, local.shape[1]), dtype=local.dtype, device=local.device)
-    dist.all_gather_into_tensor(out, buf, group=group)
-    return out[:n].contiguous()
+    return RowGather(n, local.shape[1], local.dtype, local.device, group)(local)
+
+
+def all_reduce_fp64(value, group=None):
+    """Sum of a float64 scalar (device tensor) over the ranks of `group` (energies)."""
+    v = value.to(torch.float64).reshape(1).clone()
+    dist.all_reduce(v, op=dist.ReduceOp.SUM, group=group)
+    return v[0]
 
 
 def library_step_rows(K, origin):
@@ -71,35 +93,78 @@ def library_adjoint_rows(K, origin):
     return step
 
 
-def sharded_second_order_shoot(X0, A0, timeStep, step_rows, group=None):
+def library_k_rows(K, origin):
+    """Rows r0..r1 of K(x) a on the GPU (lddmm_apply_k with the row range as targets)."""
+    sigma = float(np.asarray(K.sigma).ravel()[0])
+    o = nat.origin_arg(origin)
+
+    def k_rows(x, a, r0, r1):
+        n, nr = x.shape[0], r1 - r0
+        out = torch.empty((nr, 3), dtype=torch.float64, device=x.device)
+        if nr == 0:
+            return out
+        y = x[r0:r1].contiguous()
+        ws, wsb = nat.workspace(nr, n, K.precision)
+        nat.check(nat.lib().lddmm_apply_k(nat.ptr(y), nr, nat.ptr(x), nat.ptr(a), n, sigma, K.code, o, nat.ptr(out),
+                                          K.precision, ws, wsb, nat.stream_ptr()), 'apply_k')
+        return out
+    return k_rows
+
+
+def sharded_second_order_shoot(X0, A0, timeStep, step_rows, group=None, gather=None):
     """Geodesic shooting with the rows of every step sharded over the ranks of `group`; returns the full (xt, at)
     (T+1, n, 3) on every rank (secondOrderEvolution, base/pointEvolution.py:385-472)."""
     world, rank = dist.get_world_size(group), dist.get_rank(group)
     T = int(np.round(1.0 / timeStep))
     n = X0.shape[0]
     r0, r1 = row_range(n, world, rank)
+    gather = gather or RowGather(n, 3, X0.dtype, X0.device, group)
     xt = torch.empty((T + 1, n, 3), dtype=X0.dtype, device=X0.device)
     at = torch.empty_like(xt)
     xt[0], at[0] = X0, A0
     for t in range(T):
         x1, a1 = step_rows(xt[t], at[t], r0, r1, timeStep)
-        xt[t + 1] = all_gather_rows(x1, n, group)
-        at[t + 1] = all_gather_rows(a1, n, group)
+        gather(x1, xt[t + 1])
+        gather(a1, at[t + 1])
     return xt, at
 
 
-def sharded_second_order_adjoint(xt, at, px1, pa1, timeStep, adjoint_rows, group=None):
+def sharded_second_order_adjoint(xt, at, px1, pa1, timeStep, adjoint_rows, group=None, gather=None):
     """Adjoint sweep (secondOrderCovector, base/pointEvolution.py:489-552) with the rows of every step sharded;
     returns the full (pxt, pat) on every rank."""
     world, rank = dist.get_world_size(group), dist.get_rank(group)
     T = xt.shape[0] - 1
     n = xt.shape[1]
     r0, r1 = row_range(n, world, rank)
+    gather = gather or RowGather(n, 3, xt.dtype, xt.device, group)
     pxt = torch.empty_like(xt)
     pat = torch.empty_like(xt)
     pxt[T], pat[T] = px1, pa1
     for t in range(T - 1, -1, -1):
         p0, q0 = adjoint_rows(xt[t], at[t], pxt[t + 1], pat[t + 1], r0, r1, timeStep)
-        pxt[t] = all_gather_rows(p0, n, group)
-        pat[t] = all_gather_rows(q0, n, group)
+        gather(p0, pxt[t])
+        gather(q0, pat[t])
     return pxt, pat
+
+
+def sharded_kinetic(X0, A0, k_rows, group=None, gather=None):
+    """(0.5 a0.K(x0)a0 as an FP64 device scalar summed over the ranks, full K(x0)a0 on every rank): the kinetic term
+    of the second-order objective (base/secondOrderPointSetMatching.py:113-148) with its rows sharded."""
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    n = X0.shape[0]
+    r0, r1 = row_range(n, world, rank)
+    ka = k_rows(X0, A0, r0, r1)
+    e = all_reduce_fp64(0.5 * (A0[r0:r1] * ka).sum(), group)
+    gather = gather or RowGather(n, 3, X0.dtype, X0.device, group)
+    return e, gather(ka)
+
+
+def sharded_second_order_gradient(X0, A0, px1, timeStep, step_rows, adjoint_rows, k_rows, group=None):
+    """The second-order objective's deformation part and gradient with every sum sharded by rows: shooting, the FP64
+    kinetic energy, the adjoint sweep from the end-point covector px1 (pa1 = 0) and da0 = K(x0)a0 - pa_0
+    (base/secondOrderPointSetMatching.py:379-483). Returns (kinetic energy, xt, at, da0), identical on every rank."""
+    gather = RowGather(X0.shape[0], 3, X0.dtype, X0.device, group)
+    xt, at = sharded_second_order_shoot(X0, A0, timeStep, step_rows, group, gather)
+    e, ka0 = sharded_kinetic(X0, A0, k_rows, group, gather)
+    _, pat = sharded_second_order_adjoint(xt, at, px1, torch.zeros_like(px1), timeStep, adjoint_rows, group, gather)
+    return e, xt, at, ka0 - pat[0]

@@ -13,7 +13,8 @@ Differences from the reference, by design:
     shoots forward again inside every gradient, base/pointEvolution.py:516-519 and base/surfaceMatching.py:757);
   * the first-order kinetic energy sum_t a_t.K(x_t)a_t is read from the shooting kernels' epilogue instead of a
     second K(x_t)a_t per time step (base/surfaceMatching.py:546-548);
-  * affine parts, landmarks, symmetric / unreduced / SGD variants and file output are not implemented.
+  * affine parts, landmarks, symmetric / unreduced / SGD variants are not implemented; of the file output, the
+    result record of `saveHdf5` is written as an .npz archive with the same keys (h5py is not available).
 """
 import logging
 import time
@@ -62,7 +63,7 @@ class _DeviceMatching:
                 'affineKernel': False, 'testGradient': False, 'Landmarks': None, 'saveFile': 'evolution',
                 'saveRate': 10, 'mode': 'normal', 'verb': True, 'pplot': False, 'outputDir': '.',
                 'symmetric': False, 'internalCost': None, 'lineSearch': 'Weak_Wolfe', 'gradTol': -1.,
-                'gradLB': 0.001, 'initialMomentum': None, 'targetObjective': None}
+                'gradLB': 0.001, 'initialMomentum': None, 'targetObjective': None, 'processGroup': None}
 
     def __init__(self, Template=None, Target=None, options=None):
         self.options = self.getDefaultOptions()
@@ -245,6 +246,36 @@ class _DeviceMatching:
     def endOptim(self):
         self.fvDef.updateVertices(self.state['xt'][-1].cpu().numpy())
 
+    def saveHdf5(self, fileName):
+        """The result record of the reference's saveHdf5 (base/surfaceMatching.py:1506-1555) as an .npz archive:
+        the HDF5 group path of each dataset is its key ('LDDMM Results/parameters/Time steps', ...). Written to
+        `fileName` with its extension replaced by .npz (h5py is not available); returns that path."""
+        import os
+        o = self.options
+        K, Kd = o['KparDiff'], o['KparDist']
+        ctrl = self.control[self.control_key]
+        rec = {'parameters/Time steps': self.Tsize,
+               'parameters/Deformation Kernel type': K.name,
+               'parameters/Deformation Kernel width': np.asarray(K.sigma),
+               'parameters/Deformation Kernel order': K.order,
+               'parameters/Spatial Varifold Kernel type': Kd.name,
+               'parameters/Spatial Varifold width': np.asarray(Kd.sigma),
+               'parameters/Spatial Varifold order': Kd.order,
+               'template/vertices': self.fv0.vertices, 'template/faces': self.fv0.faces,
+               'target/vertices': self.fv1.vertices, 'target/faces': self.fv1.faces,
+               'variables/alpha': ctrl.cpu().numpy(), 'variables/affine': 'None'}
+        st = self.solveStateEquation(withJacobian=True)
+        xt = st['xt']
+        self.fvDef.updateVertices(xt[-1].cpu().numpy())
+        rec['deformedTemplate/vertices'] = self.fvDef.vertices
+        av0 = self.fv0.computeVertexArea()[0]
+        rec['descriptors/Jacobian'] = st['Jt'][-1].cpu().numpy()
+        rec['descriptors/Surface Jacobian'] = self.fvDef.computeVertexArea()[0] / av0
+        rec['descriptors/Displacement'] = (xt[-1] - xt[0]).cpu().numpy()
+        path = os.path.splitext(fileName)[0] + '.npz'
+        np.savez(path, **{'LDDMM Results/' + k: np.asarray(v) for k, v in rec.items()})
+        return path
+
     def optimizeMatching(self):
         grd = self.getGradient(self.gradCoeff)
         [grd2] = self.dotProduct_euclidean(grd, [grd])
@@ -297,11 +328,38 @@ class SurfaceMatching(_DeviceMatching):
     def randomDir(self):
         return Control(at=torch.randn((self.Tsize, self.npt, 3), dtype=torch.float64, device=self.x0.device))
 
+    def solveStateEquation(self, control=None, withJacobian=False):
+        """Trajectory (and log-Jacobian) of the control (base/surfaceMatching.py:116, landmarkDirectEvolutionEuler)."""
+        control = self.control if control is None else control
+        return evol.landmarkDirectEvolutionEuler(self.x0, control['at'], self.options['KparDiff'],
+                                                 options={'withJacobian': withJacobian})
+
 
 class SecondOrderSurfaceMatching(_DeviceMatching):
     """Geodesic-shooting surface matching (base/secondOrderSurfaceMatching.py:41,
-    base/secondOrderPointSetMatching.py:45-494)."""
+    base/secondOrderPointSetMatching.py:45-494).
+
+    options['processGroup'] (a torch.distributed group, or True for the default group; one process per GPU, every
+    rank given the same surfaces and options) shards the target rows of every shooting step, every adjoint step and
+    the kinetic term K(x0)a0 over the ranks (base/distributed.py): one all-gather of the new rows per step, an FP64
+    all-reduce of the kinetic energy. The data term is evaluated on every rank (it is 10-20% of an iteration), so
+    every rank holds the same objective, gradient and BFGS state and takes the same decisions."""
     control_key = 'a0'
+
+    def _sharding(self):
+        pg = self.options.get('processGroup')
+        if pg is None or pg is False:
+            return None
+        from . import distributed as dd
+        group = None if pg is True else pg
+        K = self.options['KparDiff']
+        key = (id(group), K.pk_dtype)
+        if getattr(self, '_shard_key', None) != key:
+            self._shard = (dd, group, dd.library_step_rows(K, self.origin), dd.library_adjoint_rows(K, self.origin),
+                           dd.library_k_rows(K, self.origin), dd.RowGather(self.npt, 3, torch.float64, self.x0.device,
+                                                                           group))
+            self._shard_key = key
+        return self._shard
 
     def initialize_variables(self):
         a0 = self.options['initialMomentum']
@@ -318,6 +376,13 @@ class SecondOrderSurfaceMatching(_DeviceMatching):
         """0.5 a0.K(x0)a0 with the geodesic trajectory (base/secondOrderPointSetMatching.py:113-148)."""
         K = self.options['KparDiff']
         a0 = control['a0']
+        sh = self._sharding()
+        if sh is not None:
+            dd, group, step_rows, _, k_rows, gather = sh
+            xt, at = dd.sharded_second_order_shoot(self.x0, a0, self.options['timeStep'], step_rows, group, gather)
+            obj, _ = dd.sharded_kinetic(self.x0, a0, k_rows, group, gather)
+            st = State(xt=xt, at=at)
+            return (obj, st) if withTrajectory or withJacobian else obj
         xt, at = evol.shoot_second_order(self.x0, a0, K, self.options['timeStep'], origin=self.origin)
         obj = 0.5 * (a0 * K._apply_k(self.x0, self.x0, a0, float(np.asarray(K.sigma).ravel()[0]), self.origin)).sum() \
             if np.asarray(K.sigma).size == 1 else 0.5 * (a0 * K.applyK(self.x0, a0)).sum()
@@ -332,6 +397,15 @@ class SecondOrderSurfaceMatching(_DeviceMatching):
             control, st = self.setUpdate(update)
         px1 = -self.endPointGradient(st['xt'][-1])
         pa1 = torch.zeros_like(px1)
+        sh = self._sharding()
+        if sh is not None:
+            dd, group, _, adjoint_rows, k_rows, gather = sh
+            _, pat = dd.sharded_second_order_adjoint(st['xt'], st['at'], px1, pa1, self.options['timeStep'],
+                                                     adjoint_rows, group, gather)
+            _, ka0 = dd.sharded_kinetic(self.x0, control['a0'], k_rows, group, gather)
+            grd = Control()
+            grd['a0'] = (ka0 - pat[0]) / coeff
+            return grd
         _, _, da0 = evol.second_order_adjoint(st['xt'], st['at'], px1, pa1, self.options['KparDiff'],
                                               self.options['timeStep'], origin=self.origin)
         grd = Control()
@@ -340,3 +414,10 @@ class SecondOrderSurfaceMatching(_DeviceMatching):
 
     def randomDir(self):
         return Control(a0=torch.randn((self.npt, 3), dtype=torch.float64, device=self.x0.device))
+
+    def solveStateEquation(self, control=None, withJacobian=False):
+        """Geodesic trajectory (and log-Jacobian) of the control (base/secondOrderPointSetMatching.py:100,
+        secondOrderEvolution)."""
+        control = self.control if control is None else control
+        return evol.secondOrderEvolution(self.x0, control['a0'], self.options['KparDiff'], self.options['timeStep'],
+                                         options={'withJacobian': withJacobian})

@@ -1,8 +1,11 @@
-"""Minimal drop-in `Surface` container (reference: base/surfaces.py:226-351, :1645-1655).
+"""Minimal drop-in `Surface` container (reference: base/surfaces.py:226-351, :364-440, :1645-1655).
 
 Holds what the point-set hot path reads: vertices, faces, vertex weights, face weights, face centres and
-surfels (cross(v2-v1, v3-v1)/2). Mesh I/O, remeshing and plotting of the reference are outside this package;
-`read_obj` / `read_vtk_ascii` cover plain triangle files.
+surfels (cross(v2-v1, v3-v1)/2), and the vertex areas of the output descriptors. Remeshing and plotting of the
+reference are outside this package; `read_obj` / `read_vtk_ascii` read plain triangle files without the vtk
+library, which the reference needs for them (base/surfaces.py:1880-1980). Like vtk's readers, which store points in
+single precision, they round coordinates declared `float` (and every OBJ coordinate) to float32 before widening
+them to float64, so a mesh read here has the vertices the reference would have.
 """
 import numpy as np
 
@@ -83,6 +86,36 @@ class Surface:
     def saveVTK(self, fileName):
         write_vtk_ascii(fileName, self.faces, self.vertices)
 
+    def computeVertexArea(self, simpleMethod=False):
+        """(vertex areas AV, face areas AF) (base/surfaces.py:364-440). simpleMethod: a third of each face's area
+        to each corner. Otherwise the mixed rule the reference uses: a face without an obtuse angle gives corner i
+        (|e_ij|^2 cot(angle at k) + |e_ik|^2 cot(angle at j)) / 8 (its Voronoi share); a face obtuse at a corner
+        gives each other corner |edge to the obtuse corner|^2 / (8 cot(own angle)) and the obtuse corner the rest."""
+        V, F = self.vertices, self.faces
+        p = [V[F[:, k]] for k in range(3)]
+        e12, e13, e23 = p[1] - p[0], p[2] - p[0], p[2] - p[1]
+        AF = np.sqrt((np.cross(e12, e13) ** 2).sum(axis=1)) / 2
+        AV = np.zeros(V.shape[0])
+        if simpleMethod:
+            for k in range(3):
+                np.add.at(AV, F[:, k], AF / 3)
+            return AV, AF
+        l12, l13, l23 = (e12 ** 2).sum(1), (e13 ** 2).sum(1), (e23 ** 2).sum(1)
+        c1 = (e12 * e13).sum(1) / np.sqrt(l12 * l13)
+        c2 = -(e12 * e23).sum(1) / np.sqrt(l12 * l23)
+        c3 = (e13 * e23).sum(1) / np.sqrt(l13 * l23)
+        cot = [c / np.sqrt(1 - c ** 2) for c in (c1, c2, c3)]
+        with np.errstate(divide='ignore', invalid='ignore'):
+            u = np.stack([(l12 * cot[2] + l13 * cot[1]) / 8, (l12 * cot[2] + l23 * cot[0]) / 8,
+                          (l13 * cot[1] + l23 * cot[0]) / 8], axis=1)
+            ob1 = np.stack([AF - l12 / (8 * cot[1]) - l13 / (8 * cot[2]), l12 / (8 * cot[1]), l13 / (8 * cot[2])], 1)
+            ob2 = np.stack([l12 / (8 * cot[0]), AF - l12 / (8 * cot[0]) - l23 / (8 * cot[2]), l23 / (8 * cot[2])], 1)
+            ob3 = np.stack([l13 / (8 * cot[0]), l23 / (8 * cot[1]), AF - l13 / (8 * cot[0]) - l23 / (8 * cot[1])], 1)
+        u = np.where((c1 < 0)[:, None], ob1, np.where((c2 < 0)[:, None], ob2, np.where((c3 < 0)[:, None], ob3, u)))
+        for k in range(3):
+            np.add.at(AV, F[:, k], u[:, k])
+        return AV, AF
+
 
 def read_obj(path):
     v, f = [], []
@@ -97,7 +130,7 @@ def read_obj(path):
                 idx = [int(t.split('/')[0]) - 1 for t in tok[1:]]
                 for k in range(1, len(idx) - 1):
                     f.append([idx[0], idx[k], idx[k + 1]])
-    return np.array(f, dtype=np.int64), np.array(v, dtype=np.float64)
+    return np.array(f, dtype=np.int64), np.array(v, dtype=np.float32).astype(np.float64)
 
 
 def read_vtk_ascii(path):
@@ -106,6 +139,8 @@ def read_vtk_ascii(path):
     i = tok.index('POINTS')
     npts = int(tok[i + 1])
     v = np.array(tok[i + 3:i + 3 + 3 * npts], dtype=np.float64).reshape(npts, 3)
+    if tok[i + 2].lower() == 'float':
+        v = v.astype(np.float32).astype(np.float64)
     j = tok.index('POLYGONS')
     nf = int(tok[j + 1])
     k = j + 3

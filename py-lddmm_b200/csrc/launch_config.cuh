@@ -17,6 +17,9 @@
 #ifndef LDDMM_RT_ADJOINT
 #define LDDMM_RT_ADJOINT 4
 #endif
+#ifndef LDDMM_RT_SYM_FWD
+#define LDDMM_RT_SYM_FWD 4
+#endif
 #ifndef LDDMM_TPB_64
 #define LDDMM_TPB_64 128
 #endif
@@ -36,6 +39,10 @@ constexpr int kRtHeavy = LDDMM_RT_HEAVY;
 // 2 CTAs per SM) measured 4% faster than 2 targets per thread at 4 CTAs per SM (half the shared-memory reads per
 // pair, two independent lane groups per source).
 constexpr int kRtAdjoint = LDDMM_RT_ADJOINT;
+// The symmetric second-order forward step (pairs_kernel_sym): 4 targets per thread (8 would need more than the
+// 48 KiB of static shared memory for its compensated row sums; the per-step shuffles and loads that more targets
+// would amortise run beside the FMA pipe, which bounds the step).
+constexpr int kRtSymFwd = LDDMM_RT_SYM_FWD;
 // FP64 baseline path.
 constexpr int kTpb64 = LDDMM_TPB_64;
 constexpr int kRt64 = LDDMM_RT_64;

@@ -37,6 +37,12 @@
 #ifndef LDDMM_SOBWD_MIN_CTAS
 #define LDDMM_SOBWD_MIN_CTAS 1  // at 4 targets per thread (LDDMM_RT_ADJOINT) no cap: 254 registers, 2 CTAs per SM
 #endif
+#ifndef LDDMM_SOBWD_SYM_MIN_CTAS
+#define LDDMM_SOBWD_SYM_MIN_CTAS 2  // the symmetric adjoint step (pairs_kernel_sym)
+#endif
+#ifndef LDDMM_SOFWD_SYM_MIN_CTAS
+#define LDDMM_SOFWD_SYM_MIN_CTAS 2  // the symmetric forward step (pairs_kernel_sym)
+#endif
 #ifndef LDDMM_FOBWD_MIN_CTAS
 #define LDDMM_FOBWD_MIN_CTAS 1
 #endif

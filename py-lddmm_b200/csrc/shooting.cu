@@ -3,6 +3,7 @@
 #include "../../include/lddmm_b200.h"
 #include "kernel_ops.cuh"
 #include "launch_config.cuh"
+#include "pairs_sym.cuh"
 
 namespace lddmm {
 
@@ -205,6 +206,131 @@ struct OpSOBwd {
   }
 };
 
+// The second-order forward step evaluated once per unordered pair (pairs_kernel_sym; Gaussian, FP32, whole steps):
+// e and c = a_k.a_l are symmetric and d changes sign, so the row sums K a (e a_l) and A (e c d) of k mirror into
+// e a_k and -e c d for l. 22 FP32 lane-ops per unordered pair (11 per ordered pair, against 14 for the expanded
+// form of OpSOFwd and 16 for its difference form), one ex2.
+struct OpSOFwdSym {
+  using Params = OpSOFwd::Params;
+  static constexpr int NSS = 6, NR = 6, NC = 6;
+  static constexpr int kSymMinCtas = LDDMM_SOFWD_SYM_MIN_CTAS;
+  struct SymTgt { F2 y0, y1, y2, a0, a1, a2; };
+  static __device__ __forceinline__ void load_target_sym(const Params& P, int i0, int i1, bool v0, bool v1,
+                                                         SymTgt& t) {
+    t.y0 = tgt_coord<F2>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<F2>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<F2>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.a0 = VT<F2>::pack(v0 ? P.a[3 * i0] : 0.0, v1 ? P.a[3 * i1] : 0.0);
+    t.a1 = VT<F2>::pack(v0 ? P.a[3 * i0 + 1] : 0.0, v1 ? P.a[3 * i1 + 1] : 0.0);
+    t.a2 = VT<F2>::pack(v0 ? P.a[3 * i0 + 2] : 0.0, v1 ? P.a[3 * i1 + 2] : 0.0);
+  }
+  // fields: x' (0-2), a (3-5)
+  static __device__ __forceinline__ void source_fields_sym(const Params& P, int l, double* f) {
+    OpSOFwd::source_fields(P, l, f);
+  }
+  template <bool COL>
+  static __device__ __forceinline__ void pair_sym(const Frame&, const SymTgt& t, const F2* s, F2* row, F2* col) {
+    const F2 d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const F2 e = VT<F2>::expneg(sqdist(d0, d1, d2));
+    const F2 ec = e * dot3(t.a0, t.a1, t.a2, s[3], s[4], s[5]);
+    row[0] = fma(e, s[3], row[0]);
+    row[1] = fma(e, s[4], row[1]);
+    row[2] = fma(e, s[5], row[2]);
+    row[3] = fma(ec, d0, row[3]);
+    row[4] = fma(ec, d1, row[4]);
+    row[5] = fma(ec, d2, row[5]);
+    if constexpr (COL) {
+      col[0] = fma(e, t.a0, col[0]);
+      col[1] = fma(e, t.a1, col[1]);
+      col[2] = fma(e, t.a2, col[2]);
+      col[3] = fma(ec, d0, col[3]);
+      col[4] = fma(ec, d1, col[4]);
+      col[5] = fma(ec, d2, col[5]);
+    }
+  }
+  // K a = row + col; sum e c d = row - col (the mirrored difference changes sign)
+  static __device__ __forceinline__ void finalize_sym(const Params& P, int i, const double* row, const double* col) {
+    const double ka = P.dt * P.f.kappa;
+    for (int c = 0; c < 3; ++c) {
+      P.x1[3 * i + c] = P.x[3 * i + c] + P.dt * (row[c] + col[c]);
+      P.a1[3 * i + c] = P.a[3 * i + c] + ka * (row[3 + c] - col[3 + c]);
+    }
+  }
+};
+
+// The second-order adjoint step evaluated once per unordered pair (pairs_kernel_sym; Gaussian, FP32, whole steps).
+// Every per-pair quantity of OpSOBwd is symmetric in (k, l) or changes sign: e, c1 = px'_k.a_l + a_k.px'_l,
+// c2 = b_k.a_l (b = -kappa^2 a) and dq = d.(pa_k - pa_l) are symmetric, d and w = pa_k - pa_l change sign. With the
+// four sums merged pairwise (as the epilogue of OpSOBwd combines them),
+//   row px-sum of k:  v = eg d + cd ec2 w          (eg = e (c1 + c2 dq), ec2 = e c2, cd = -1/(kappa^2 sigma^2))
+//   row pa-sum of k:  e px'_l - kappa^2 edq a_l    (edq = e dq)
+// the mirrored contributions to l are -v and e px'_k + edq b_k. 51 FP32 lane-ops per unordered pair (25.5 per
+// ordered pair, against 37 for OpSOBwd), one ex2.
+struct OpSOBwdSym {
+  using Params = OpSOBwd::Params;
+  static constexpr int NSS = 12, NR = 6, NC = 6;
+  static constexpr int kSymMinCtas = LDDMM_SOBWD_SYM_MIN_CTAS;
+  struct SymTgt { F2 y0, y1, y2, a0, a1, a2, b0, b1, b2, p0, p1, p2, q0, q1, q2, cd, k2; };
+  static __device__ __forceinline__ void load_target_sym(const Params& P, int i0, int i1, bool v0, bool v1,
+                                                         SymTgt& t) {
+    const double k = P.f.kappa;
+    auto fld = [&](const double* a, int c, double sc) {
+      return VT<F2>::pack(v0 ? sc * a[3 * i0 + c] : 0.0, v1 ? sc * a[3 * i1 + c] : 0.0);
+    };
+    t.y0 = tgt_coord<F2>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<F2>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<F2>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.a0 = fld(P.a, 0, 1.0); t.a1 = fld(P.a, 1, 1.0); t.a2 = fld(P.a, 2, 1.0);
+    t.b0 = fld(P.a, 0, -k * k); t.b1 = fld(P.a, 1, -k * k); t.b2 = fld(P.a, 2, -k * k);
+    t.p0 = fld(P.px, 0, -k); t.p1 = fld(P.px, 1, -k); t.p2 = fld(P.px, 2, -k);
+    t.q0 = fld(P.pa, 0, 1.0); t.q1 = fld(P.pa, 1, 1.0); t.q2 = fld(P.pa, 2, 1.0);
+    t.cd = VT<F2>::dup(-P.f.inv_s2 / (k * k));
+    t.k2 = VT<F2>::dup(-k * k);
+  }
+  // fields: x' (0-2), a (3-5), pa (6-8), px' = -kappa px (9-11)
+  static __device__ __forceinline__ void source_fields_sym(const Params& P, int l, double* f) {
+    OpSOBwd::source_fields(P, l, f);
+  }
+  template <bool COL>
+  static __device__ __forceinline__ void pair_sym(const Frame&, const SymTgt& t, const F2* s, F2* row, F2* col) {
+    const F2 d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const F2 e = VT<F2>::expneg(sqdist(d0, d1, d2));
+    const F2 w0 = t.q0 - s[6], w1 = t.q1 - s[7], w2 = t.q2 - s[8];
+    const F2 dq = dot3(d0, d1, d2, w0, w1, w2);
+    const F2 c1 = fma(t.a2, s[11], fma(t.a1, s[10], fma(t.a0, s[9], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
+    const F2 ec2 = e * dot3(t.b0, t.b1, t.b2, s[3], s[4], s[5]);
+    const F2 eg = fma(ec2, dq, e * c1);
+    const F2 tw = ec2 * t.cd;
+    const F2 v0 = fma(tw, w0, eg * d0), v1 = fma(tw, w1, eg * d1), v2 = fma(tw, w2, eg * d2);
+    row[0] += v0;
+    row[1] += v1;
+    row[2] += v2;
+    const F2 edq = e * dq;
+    const F2 edqk = edq * t.k2;
+    row[3] = fma(edqk, s[3], fma(e, s[9], row[3]));
+    row[4] = fma(edqk, s[4], fma(e, s[10], row[4]));
+    row[5] = fma(edqk, s[5], fma(e, s[11], row[5]));
+    if constexpr (COL) {
+      col[0] += v0;
+      col[1] += v1;
+      col[2] += v2;
+      col[3] = fma(edq, t.b0, fma(e, t.p0, col[3]));
+      col[4] = fma(edq, t.b1, fma(e, t.p1, col[4]));
+      col[5] = fma(edq, t.b2, fma(e, t.p2, col[5]));
+    }
+  }
+  // zpx = row - col (the mirrored px-sum changes sign), zpa = -(row + col) / kappa
+  static __device__ __forceinline__ void finalize_sym(const Params& P, int i, const double* row, const double* col) {
+    const double k = P.f.kappa;
+    for (int c = 0; c < 3; ++c) {
+      const double zpx = row[c] - col[c];
+      const double zpa = -(row[3 + c] + col[3 + c]) / k;
+      P.px_prev[3 * i + c] = P.px[3 * i + c] + P.dt * zpx;
+      P.pa_prev[3 * i + c] = P.pa[3 * i + c] + P.dt * zpa;
+    }
+  }
+};
+
 // First-order adjoint step with the gradient of the same step (base/pointEvolution.py:186-201, :221-223;
 // base/surfaceMatching.py:810, :879-891):
 //   p_t = p_{t+1} + dt DK^T_lddmm(x_t; p_{t+1}, a_t) = p_{t+1} - dt kappa sum_l e (p_k.a_l + a_k.q_l) d,
@@ -268,6 +394,10 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
   size_t b = 0;
   auto upd = [&](size_t v) { b = v > b ? v : b; };
   if (precision == kFP32Compensated) {
+    if (LDDMM_SYM) {
+      upd(sym_ws_bytes<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(n));
+      upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymFwd>(n));
+    }
     upd(pairs_ws_bytes_any<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
     upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtAdjoint, Gauss>(n, n));
     upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtHeavy, Laplacian>(n, n));
@@ -334,7 +464,11 @@ template <typename V>
 int so_step(const double* x, const double* a, int64_t n, const Frame& f, double dt, double* x1, double* a1, void* ws,
             size_t wsb, cudaStream_t st, int64_t row0 = 0, int64_t nrows = -1) {
   OpSOFwd::Params P{x, a, x1, a1, f, dt, (int)row0};
-  return run_pairs_k<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, nrows < 0 ? n : nrows, n, ws, wsb, st);
+  const int64_t rows = nrows < 0 ? n : nrows;
+  if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
+    if (f.family == kGauss && row0 == 0 && rows == n) return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymFwd>(P, n, ws, wsb, st);
+  }
+  return run_pairs_k<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, rows, n, ws, wsb, st);
 }
 
 template <typename V>
@@ -343,6 +477,9 @@ int so_adjoint_step(const double* x, const double* a, const double* px, const do
                     int64_t row0 = 0, int64_t nrows = -1) {
   OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt, (int)row0};
   const int64_t rows = nrows < 0 ? n : nrows;
+  if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
+    if (f.family == kGauss && row0 == 0 && rows == n) return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(P, n, ws, wsb, st);
+  }
   if (f.family == kGauss) return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH, Gauss>(P, rows, n, ws, wsb, st);
   return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtHL, Laplacian>(P, rows, n, ws, wsb, st);
 }

@@ -1,5 +1,6 @@
-"""Row-sharded shooting and adjoint (base/distributed.py) on world-size-2 `gloo` ranks on the CPU, with the oracle's
-float64 sums as the per-rank step: the gathered trajectories equal the single-process oracle trajectories."""
+"""Row-sharded shooting, adjoint and second-order gradient (base/distributed.py) on world-size-2 `gloo` ranks on the
+CPU, with the oracle's float64 sums as the per-rank steps: the gathered trajectories, the gradient da0 and the
+all-reduced kinetic energy equal the single-process oracle's."""
 import os
 import sys
 
@@ -31,6 +32,12 @@ def _oracle_steps():
     return step, adjoint
 
 
+def _oracle_k_rows(x, a, r0, r1):
+    import oracle as O
+    X, A = x.numpy(), a.numpy()
+    return torch.from_numpy(O.apply_k(X[r0:r1], X, A, SIGMA))
+
+
 def _worker(rank, world, port, x0, a0, px1, result_path):
     for p in (REPO, PKG):
         if p not in sys.path:
@@ -45,8 +52,11 @@ def _worker(rank, world, port, x0, a0, px1, result_path):
         X0, A0 = torch.from_numpy(x0), torch.from_numpy(a0)
         xt, at = dd.sharded_second_order_shoot(X0, A0, DT, step)
         pxt, pat = dd.sharded_second_order_adjoint(xt, at, torch.from_numpy(px1), torch.zeros_like(X0), DT, adjoint)
+        e, _, _, da0 = dd.sharded_second_order_gradient(X0, A0, torch.from_numpy(px1), DT, step, adjoint,
+                                                        _oracle_k_rows)
         if rank == 0:
-            np.savez(result_path, xt=xt.numpy(), at=at.numpy(), pxt=pxt.numpy(), pat=pat.numpy())
+            np.savez(result_path, xt=xt.numpy(), at=at.numpy(), pxt=pxt.numpy(), pat=pat.numpy(), da0=da0.numpy(),
+                     kinetic=float(e))
         # every rank holds the same gathered trajectory
         h = torch.tensor([float(xt.sum()), float(pxt.sum())], dtype=torch.float64)
         hs = [torch.zeros_like(h) for _ in range(world)]
@@ -76,5 +86,6 @@ def test_sharded_shooting_gloo_world2(tmp_path):
     mp.start_processes(_worker, args=(2, port, x0, a0, px1, out), nprocs=2, join=True, start_method='spawn')
     r = np.load(out)
     ref = O.second_order_gradient(x0, a0, px1, np.zeros_like(x0), SIGMA, DT)
-    for k in ('xt', 'at', 'pxt', 'pat'):
+    for k in ('xt', 'at', 'pxt', 'pat', 'da0'):
         assert np.allclose(r[k], ref[k], rtol=1e-12, atol=1e-12), k
+    assert np.isclose(float(r['kinetic']), 0.5 * (a0 * O.apply_k(x0, x0, a0, SIGMA)).sum(), rtol=1e-13)

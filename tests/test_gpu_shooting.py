@@ -186,3 +186,76 @@ def test_sharded_shooting_nccl_single_rank():
         dist.destroy_process_group()
     rx, ra = evol.shoot_second_order(X, A, K, 0.1, origin=o)
     assert torch.equal(xt, rx) and torch.equal(at, ra)
+
+
+@pytest.mark.parametrize('n', [1, 2, 33, 129, 511, 512, 513, 1025, 2049, 5000])
+def test_symmetric_adjoint_step_ragged_sizes(n):
+    """The whole-step FP32 Gaussian adjoint step evaluates each unordered pair once (pairs_kernel_sym). It must agree
+    with the ordered-pair kernel (the same step computed as two row ranges) and with the FP64 oracle at sizes that
+    leave partial blocks and tiles, a single block, and blocks whose column partials come from many rows."""
+    import torch
+    import oracle as O
+    from base import distributed as dd
+    from base import _native as nat
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1, 1, (n, 3))
+    a = rng.normal(0, 0.1, (n, 3))
+    px = rng.normal(size=(n, 3))
+    pa = rng.normal(0, 0.1, (n, 3))
+    X, A, PX, PA = (torch.from_numpy(v).cuda() for v in (x, a, px, pa))
+    K = kernel(0.5, 'float32')
+    o = nat.centroid(X)
+    adj = dd.library_adjoint_rows(K, o)
+    dt = 0.05
+    p_sym, q_sym = adj(X, A, PX, PA, 0, n, dt)
+    h = n // 2
+    parts = [adj(X, A, PX, PA, r0, r1, dt) for r0, r1 in ((0, h), (h, n)) if r1 > r0]
+    p_ord = torch.cat([p for p, _ in parts])
+    q_ord = torch.cat([q for _, q in parts])
+    zpx, zpa = O.second_order_adjoint_step_rows(x, a, px, pa, np.arange(n), 0.5)
+    for got, ref_o, base in ((p_sym, p_ord, px), (q_sym, q_ord, pa)):
+        inc, inc_o = (got.cpu().numpy() - base) / dt, (ref_o.cpu().numpy() - base) / dt
+        assert rel_err(inc, inc_o) < 2e-5
+    assert rel_err((p_sym.cpu().numpy() - px) / dt, zpx) < 2e-5
+    assert rel_err((q_sym.cpu().numpy() - pa) / dt, zpa) < 2e-5
+
+
+def test_sharded_matching_nccl_single_rank():
+    """SecondOrderSurfaceMatching with options['processGroup'] (the sharded rows, gathers and FP64 all-reduce on
+    NCCL, world size 1) gives the same objective and gradient as the unsharded driver."""
+    import os
+    import torch
+    import torch.distributed as dist
+    from base.kernelFunctions import Kernel
+    from base.surfaceMatching import SecondOrderSurfaceMatching
+    from base.surfaces import Surface
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    x0, F = icosphere(3)
+    x1 = bumpy_ellipsoid(x0, seed=0)
+    a0 = np.random.default_rng(10).normal(0, 0.02, x0.shape)
+
+    def make(pg):
+        K = Kernel(name='gauss', sigma=0.5)
+        K.pk_dtype = 'float32'
+        opts = dict(maxIter=2, affine='none', KparDiff=K, KparDist=('gauss', 0.3), errorType='varifold',
+                    pk_dtype='float32', timeStep=0.1, verb=False, initialMomentum=a0, processGroup=pg)
+        return SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)), options=opts)
+
+    os.environ.setdefault('MASTER_ADDR', '127.0.0.1')
+    os.environ.setdefault('MASTER_PORT', str(29900 + os.getpid() % 90))
+    dist.init_process_group('nccl', rank=0, world_size=1)
+    try:
+        fs = make(True)
+        obj_s = fs.objectiveFun()
+        g_s = fs.getGradient(1.0)['a0'].clone()
+        fs.optimizeMatching()
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    fu = make(None)
+    obj_u = fu.objectiveFun()
+    g_u = fu.getGradient(1.0)['a0']
+    fu.optimizeMatching()
+    assert abs(obj_s - obj_u) <= 1e-12 * abs(obj_u)
+    assert rel_err(g_s.cpu().numpy(), g_u.cpu().numpy()) < 1e-12
+    assert abs(fs.history[-1] - fu.history[-1]) <= 1e-10 * abs(fu.history[-1])
