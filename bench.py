@@ -63,6 +63,10 @@ SIGMAS = (0.25, 0.5)
 OPS_FP32_PER_PAIR = 6
 OPS_SFU_PER_PAIR = 1
 METRIC = 'Gauss kernel pairs/s'
+# Coarse-to-fine warm start of the registrations: the coarse levels (icosphere levels of the source) and the
+# relative objective decrease over 3 iterations below which a coarse level hands over to the next
+COARSE_LEVELS = (4, 5)
+COARSE_RTOL = 1e-4
 # The reference's own numba applyK (ku.applyK_numba, float64) at N = M = 40,962: 22.2 s per call on 8 threads of an
 # Intel Xeon at 2.70 GHz, measured by importing the reference tree (which this benchmark does not read at run time).
 REFERENCE_NUMBA_APPLYK = {'value': 7.56e7, 'unit': 'pairs/s', 'cores': 8,
@@ -371,15 +375,21 @@ def _matching(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=None, maxIt
 
 
 def _register(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=None, model=None, scales=(0.5, 0.75, 1.0),
-              maxIter=600, a0=None):
+              maxIter=600, a0=None, coarse=None, coarse_rtol=COARSE_RTOL):
     """One registration, timed from construction to the end (device synchronised): (matching, t0, seconds,
-    warm-start record). With `target`, BFGS stops at the end of the first iteration at or below it."""
+    warm-start record). With `target`, BFGS stops at the end of the first iteration at or below it. With `coarse`
+    (coarser triangulations (faces, vertices) of the source, coarsest first) the warm start is the coarse-to-fine one
+    (learnedProposal.multilevel_warm_start, with the network at the coarsest level when `model` is given);
+    otherwise the network's proposal at this level (learnedProposal.warm_start) when `model` is given."""
     import torch
     from base import learnedProposal as lp
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     f = _matching(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=target, maxIter=maxIter, a0=a0)
-    used = lp.warm_start(f, model, scales=scales) if model is not None else None
+    if coarse is not None:
+        used = lp.multilevel_warm_start(f, model, coarse, rtol=coarse_rtol, scales=scales)
+    else:
+        used = lp.warm_start(f, model, scales=scales) if model is not None else None
     f.optimizeMatching()
     torch.cuda.synchronize()
     return f, t0, time.perf_counter() - t0, used
@@ -460,18 +470,57 @@ def heldout_registrations(model, heldset, count, tol=1e-3):
             'all_reached': all(r['reached'] for r in rows)}
 
 
+def heldout_ellipsoids(model, seeds, level, coarse, tol=1e-3):
+    """Registrations of bumpy ellipsoids of other seeds (never the headline problem's seed 0), level `level`, sigma 0.5
+    / varifold 0.2, T = 20: E* and the plain FP64 time to tolerance from the FP64 run to the stopping rule, then the
+    plain FP32 path and the learned coarse-to-fine warm start to E* (1 + tol)."""
+    import torch
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    x0, F = icosphere(level)
+    rows = []
+    for seed in seeds:
+        x1 = bumpy_ellipsoid(x0, seed=seed)
+        f64, t0, _, _ = _register(x0, F, x1, 'float64', 0.5, 0.2, 0.05)
+        estar = f64.history[-1]
+        target = estar * (1 + tol)
+        it64, s64 = _first_within(f64, t0, target)
+        del f64
+        f32, _, s32, _ = _register(x0, F, x1, 'float32', 0.5, 0.2, 0.05, target=target)
+        fl, _, sl, rec = _register(x0, F, x1, 'float32', 0.5, 0.2, 0.05, target=target, model=model, coarse=coarse)
+        rows.append({'seed': seed, 'estar': estar, 'plain_fp64_iters': it64, 'plain_fp64_s': s64,
+                     'plain_fp32_iters': len(f32.history), 'plain_fp32_s': s32, 'learned_multilevel_fine_iters':
+                     len(fl.history), 'learned_multilevel_s': sl, 'reached': bool(f32.reached_target and
+                                                                                fl.reached_target),
+                     'coarse_iters': [lv['iters'] for lv in rec['levels']], 'speedup_learned_vs_plain_fp64':
+                     s64 / sl if s64 else None})
+        del f32, fl
+        torch.cuda.empty_cache()
+    sp = [r['speedup_learned_vs_plain_fp64'] for r in rows if r['speedup_learned_vs_plain_fp64']]
+    return {'problem': f'icosphere L{level} -> bumpy ellipsoids (8 bumps) of seeds {list(seeds)}, sigma 0.5 / '
+                       'varifold 0.2, T=20', 'pairs': rows,
+            'speedup_min': min(sp) if sp else None, 'speedup_geomean': float(np.exp(np.mean(np.log(sp)))) if sp
+            else None}
+
+
 def run_registration(args):
     """Seconds per registration pair to reach (E - E*)/E* <= 1e-3 on the level-6 icosphere -> bumpy ellipsoid problem
-    (Gaussian sigma 0.5, varifold sigma 0.2, T = 20, sigmaError 1, BFGS): plain FP64 path, FP32 path, and FP32 path
-    with the learned warm start (network trained here at level 4 on pairs generated by shooting)."""
+    (Gaussian sigma 0.5, varifold sigma 0.2, T = 20, sigmaError 1, BFGS): the plain FP64 path, the plain FP32 path,
+    the FP32 path from the network's proposal at level 6, the FP32 path from the coarse-to-fine warm start without
+    the network, and the learned warm start proper (network proposal at the coarsest level, plain BFGS at the
+    coarse levels, prolongation; network trained here at level 4 on pairs generated by shooting)."""
     import torch
     from base.syntheticShapes import icosphere, bumpy_ellipsoid
     level, tol = args.reg_level, 1e-3
     x0, F = icosphere(level)
     x1 = bumpy_ellipsoid(x0, seed=0)
     sig, sigd, ts = 0.5, 0.2, 0.05
+    coarse = [icosphere(lc)[::-1] for lc in COARSE_LEVELS if lc < level]
     res = {'problem': f'icosphere L{level} ({x0.shape[0]} vertices) -> bumpy ellipsoid (8 bumps), sigma {sig} / '
-                      f'varifold {sigd}, T={int(round(1 / ts))}, sigmaError 1, BFGS', 'criterion': '(E - E*)/E* <= 1e-3'}
+                      f'varifold {sigd}, T={int(round(1 / ts))}, sigmaError 1, BFGS', 'criterion': '(E - E*)/E* <= 1e-3',
+           'warm_start': {'coarse_levels': [lc for lc in COARSE_LEVELS if lc < level], 'coarse_rtol': COARSE_RTOL,
+                          'coarse_stop': 'relative objective decrease over 3 iterations below coarse_rtol',
+                          'prolongation': 'momentum density interpolated by a normalised Gaussian of 0.4 x the '
+                                          'coarse mean edge length'}}
     # E*: the plain FP64 path run to the reference's stopping rule (|obj - obj_old| < 1e-7 after burn-in); its time
     # to tolerance is that of the same run's first iterate within tolerance
     f64, t0_64, s64_total, _ = _register(x0, F, x1, 'float64', sig, sigd, ts, maxIter=args.estar_iters)
@@ -487,19 +536,32 @@ def run_registration(args):
     del f64
     torch.cuda.empty_cache()
     model, res['proposal'], heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
-    for name, dtype, model_ in (('plain_fp32', 'float32', None), ('learned_fp32', 'float32', model)):
-        f, t0, t, used = _register(x0, F, x1, dtype, sig, sigd, ts, target=target, model=model_)
+    runs = (('plain_fp32', None, None), ('learned_fp32', model, None), ('multilevel_plain_fp32', None, coarse),
+            ('learned_multilevel_fp32', model, coarse))
+    for name, model_, coarse_ in runs:
+        f, t0, t, used = _register(x0, F, x1, 'float32', sig, sigd, ts, target=target, model=model_, coarse=coarse_)
         e = _fp64_energy(f)
         res[name] = {'s_per_pair': t, 'iters': len(f.history), 'reached': bool(f.reached_target),
                      'rel_energy_fp64': (e - estar) / abs(estar)}
-        if used is not None:
+        if coarse_ is not None:
+            res[name].update({'fine_iters': len(f.history), 'coarse_iters': [lv['iters'] for lv in used['levels']],
+                              'network_proposal_used': used['network_proposal_used'],
+                              'prolonged_used': used['prolonged_used'],
+                              'rel_obj_prolonged': (used['obj_prolonged'] - estar) / abs(estar)})
+        elif used is not None:
             res[name].update({'proposal_used': used[0], 'obj_proposal': used[1], 'obj_zero': used[2],
                               'scale': used[3]})
         del f
         torch.cuda.empty_cache()
-    res['speedup_learned_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['learned_fp32']['s_per_pair']
-    res['speedup_plain_fp32_vs_plain_fp64'] = res['plain_fp64']['s_per_pair'] / res['plain_fp32']['s_per_pair']
+    p64 = res['plain_fp64']['s_per_pair']
+    res['speedup_learned_vs_plain_fp64'] = p64 / res['learned_multilevel_fp32']['s_per_pair']
+    res['speedup_learned_single_level_vs_plain_fp64'] = p64 / res['learned_fp32']['s_per_pair']
+    res['speedup_multilevel_plain_vs_plain_fp64'] = p64 / res['multilevel_plain_fp32']['s_per_pair']
+    res['speedup_plain_fp32_vs_plain_fp64'] = p64 / res['plain_fp32']['s_per_pair']
     res['heldout'] = heldout_registrations(model, heldset, args.heldout_eval)
+    seeds = [int(v) for v in args.heldout_seeds.split(',') if v.strip()] if args.heldout_seeds else []
+    if seeds:
+        res['heldout_ellipsoids'] = heldout_ellipsoids(model, seeds, level, coarse, tol)
     res['level4_fp64_50it'] = run_level4_fp64()
     return res
 
@@ -886,6 +948,7 @@ def main():
     ap.add_argument('--train-pairs', type=int, default=20000, help='pairs generated (trained on + held out)')
     ap.add_argument('--heldout-pairs', type=int, default=2000)
     ap.add_argument('--heldout-eval', type=int, default=8, help='held-out pairs registered with and without the net')
+    ap.add_argument('--heldout-seeds', default='1,2', help='bumpy-ellipsoid seeds registered as held-out problems')
     ap.add_argument('--train-epochs', type=int, default=4)
     # mode ops / registration-profile / large-registration
     ap.add_argument('--level', type=int, default=6)

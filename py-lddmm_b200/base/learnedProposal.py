@@ -307,3 +307,104 @@ def warm_start(matching, model, scales=(1.0,)):
     if used:
         matching.acceptVarTry()
     return used, obj_prop, obj_zero, best_scale
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Coarse-to-fine warm start
+# ---------------------------------------------------------------------------------------------------------------
+def mean_edge_length(vertices, faces):
+    """Mean edge length of a triangulation (each interior edge counted twice, which does not change the mean of a
+    closed mesh)."""
+    v = np.asarray(vertices, dtype=np.float64)
+    f = np.asarray(faces, dtype=np.int64)
+    e = np.concatenate([v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 1]], v[f[:, 0]] - v[f[:, 2]]])
+    return float(np.linalg.norm(e, axis=1).mean())
+
+
+def prolong_momentum(x_coarse, a_coarse, x_fine, Kdef, width):
+    """Momentum `a_coarse` on a coarse sampling of the source surface -> momentum on a finer sampling of the same
+    surface with the same velocity field to first order. The momentum density m = a * mass (mass_k = sum_l
+    K(x_k, x_l) under the deformation kernel Kdef; m has velocity units and does not depend on the sampling) is
+    interpolated at the fine points by a normalised Gaussian of `width` (a fraction of the coarse edge length keeps
+    it from smoothing the coarse solution) and divided by the fine kernel mass."""
+    Xc, Xf = nat.as_device(x_coarse), nat.as_device(x_fine)
+    m = nat.as_device(a_coarse) * kernel_mass(Kdef, Xc)
+    Kh = Kernel(name='gauss', sigma=float(width))
+    Kh.pk_dtype = 'float32'
+    num = Kh.applyK(Xc, torch.cat([m, torch.ones_like(m[:, :1])], dim=1), firstVar=Xf)
+    return (num[:, :3] / num[:, 3:4] / kernel_mass(Kdef, Xf)).contiguous()
+
+
+class _CoarseConverged(Exception):
+    pass
+
+
+def _refine(matching, rtol, window):
+    """The plain optimiser on `matching` until its objective decreases by less than `rtol` (relative) over `window`
+    iterations, or its own stopping rule, or options['maxIter']."""
+    end = matching.endOfIteration
+
+    def end_of_iteration(endP=False):
+        end(endP)
+        h = matching.history
+        if not endP and len(h) > window and (h[-1 - window] - h[-1]) <= rtol * abs(h[-1]):
+            raise _CoarseConverged()
+
+    matching.endOfIteration = end_of_iteration
+    try:
+        matching.optimizeMatching()
+    except _CoarseConverged:
+        pass
+    finally:
+        matching.endOfIteration = end
+
+
+def multilevel_warm_start(matching, model, coarse_templates, rtol=1e-4, window=3, max_iter=200, width_factor=0.4,
+                          scales=(0.5, 0.75, 1.0)):
+    """The learned warm start refined coarse to fine, for a SecondOrderSurfaceMatching `matching` (not yet
+    optimised).
+
+    `coarse_templates`: coarser triangulations (faces, vertices) of the same source surface, coarsest first. At the
+    coarsest level the network (`model`; None for none) proposes a0 and `warm_start` keeps it when it lowers that
+    level's objective; at every coarse level the plain optimiser (the same BFGS and objective, against the
+    full-resolution target) refines the momentum until the objective decreases by less than `rtol` over `window`
+    iterations (or `max_iter`), and `prolong_momentum` carries it to the next level (interpolation width
+    `width_factor` x the coarse mean edge length). At the level of `matching` the prolonged momentum is the
+    proposal: it becomes the control when it lowers the objective (the plain optimiser's zero start is the fallback),
+    and `matching.optimizeMatching()` then refines from there.
+
+    Returns a record: per level its vertex count, iterations and objective, whether the network's proposal was
+    taken, and whether the fine level took the prolonged momentum."""
+    from .surfaceMatching import SecondOrderSurfaceMatching
+    from copy import deepcopy
+    o = matching.options
+    target = (matching.fv1.faces, matching.fv1.vertices)
+    rec = {'levels': [], 'network_proposal_used': None}
+    a_prev, x_prev, h_prev = None, None, None
+    for faces, verts in coarse_templates:
+        opts = dict(o)
+        opts.update(KparDiff=deepcopy(o['KparDiff']), KparDist=deepcopy(o['KparDist']), maxIter=max_iter,
+                    targetObjective=None, verb=False, processGroup=None,
+                    initialMomentum=None if a_prev is None else prolong_momentum(x_prev, a_prev, verts,
+                                                                                  o['KparDiff'], h_prev))
+        level = SecondOrderSurfaceMatching(Template=(faces, verts), Target=target, options=opts)
+        if a_prev is None and model is not None:
+            rec['network_proposal_used'] = warm_start(level, model, scales=scales)[0]
+        _refine(level, rtol, window)
+        a_prev, x_prev = level.control['a0'], np.asarray(verts, dtype=np.float64)
+        h_prev = width_factor * mean_edge_length(verts, faces)
+        rec['levels'].append({'vertices': int(x_prev.shape[0]), 'iters': len(level.history),
+                              'objective': float(level.obj) if level.obj is not None else None})
+        del level
+    if a_prev is None:
+        rec['prolonged_used'] = False
+        return rec
+    a_fine = prolong_momentum(x_prev, a_prev, matching.x0, o['KparDiff'], h_prev)
+    matching.obj = None
+    obj_here = matching.objectiveFun()
+    o_try = matching.updateTry({'a0': matching.control['a0'] - a_fine}, 1.0, obj_here)
+    used = bool(np.isfinite(o_try) and o_try < obj_here)
+    if used:
+        matching.acceptVarTry()
+    rec.update(prolonged_used=used, obj_prolonged=float(o_try), obj_start=float(obj_here))
+    return rec

@@ -85,6 +85,25 @@ struct OpK {
   }
 };
 
+// K(x, x) a evaluated once per unordered pair (pairs_kernel_symx; Gaussian, FP32, targets == sources): the row sum
+// of k takes e_kl a_l and the column sum of l takes e_kl a_k; out_k = row_k + col_k. 9 FP32 lane-ops and one ex2
+// per unordered pair in the expanded-distance form. The epilogue options of OpK (base, scale, dots) apply.
+struct OpKSym {
+  using Params = OpK::Params;
+  static constexpr int NP = 3, NR = 3, NC = 3;
+  static constexpr int kSymMinCtas = LDDMM_KSYM_MIN_CTAS;
+  static __device__ __forceinline__ void point(const Params& P, int i, double* c) {
+    c[0] = P.x[3 * i]; c[1] = P.x[3 * i + 1]; c[2] = P.x[3 * i + 2];
+  }
+  static __device__ __forceinline__ void payload(const Params& P, int i, double* p) {
+    p[0] = P.a[3 * i]; p[1] = P.a[3 * i + 1]; p[2] = P.a[3 * i + 2];
+  }
+  static __device__ __forceinline__ void finalize_sym(const Params& P, int i, const double* row, const double* col) {
+    const double acc[3] = {row[0] + col[0], row[1] + col[1], row[2] + col[2]};
+    OpK::finalize(P, i, acc);
+  }
+};
+
 // DK^T(y, x; p, a) -- base/kernelFunctions_util.py:773-793 with gauss_fun_diffT (:233).
 //   MODE 0 (plain): c = p_k.a_l                         13 FP32 + 1 SFU
 //   MODE 1 (sym)  : c = p_k.a_l + a_k.p_l               16 FP32 + 1 SFU

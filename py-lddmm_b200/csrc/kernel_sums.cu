@@ -3,6 +3,7 @@
 #include "../../include/lddmm_b200.h"
 #include "kernel_ops.cuh"
 #include "launch_config.cuh"
+#include "pairs_sym.cuh"
 
 namespace lddmm {
 
@@ -19,9 +20,9 @@ int device_sm_count() {
   return sms;
 }
 
-int resident_ctas(const void* kernel, int threads) {
+int resident_ctas(const void* kernel, int threads, size_t dynamic_smem) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, dynamic_smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -82,6 +83,7 @@ size_t kernel_sums_ws_bytes(int64_t n, int64_t m, int precision) {
   upd(op_ws<OpDiffK1and2, kTpbLight, kRtLight>(n, m, precision));
   upd(op_ws<OpDiv, kTpbLight, kRtLight>(n, m, precision));
   upd(op_ws<OpKTensor, kTpbLight, kRtLight>(n, m, precision));
+  if (LDDMM_SYM && precision == kFP32Compensated && n == m) upd(symx_ws_bytes<OpKSym, kTpbLight, kRtKSym>(n));
   return b;
 }
 
@@ -95,6 +97,13 @@ int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, 
                   const double* origin, double* out, int precision, void* ws, size_t wsb, lddmm_stream_t stream) {
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(x, m) || bad_ptr(a, m))
     return kInvalidArgument;
+  // a self-sum K(x, x) a (the same point array as targets and sources): each unordered pair once
+  if (LDDMM_SYM && precision == kFP32Compensated && kernel == kGauss && y == x && n == m) {
+    OpK::Params P;
+    P.f = make_frame(origin, sigma, kernel, true);
+    P.y = y; P.x = x; P.a = a; P.out = out;
+    return run_pairs_symx<OpKSym, kTpbLight, kRtKSym>(P, n, ws, wsb, (cudaStream_t)stream);
+  }
   return dispatch<OpK, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, (cudaStream_t)stream,
                                             [&](OpK::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });
 }

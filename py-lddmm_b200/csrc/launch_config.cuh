@@ -18,7 +18,10 @@
 #define LDDMM_RT_ADJOINT 4
 #endif
 #ifndef LDDMM_RT_SYM_FWD
-#define LDDMM_RT_SYM_FWD 4
+#define LDDMM_RT_SYM_FWD 8
+#endif
+#ifndef LDDMM_RT_KSYM
+#define LDDMM_RT_KSYM 8
 #endif
 #ifndef LDDMM_TPB_64
 #define LDDMM_TPB_64 128
@@ -39,10 +42,13 @@ constexpr int kRtHeavy = LDDMM_RT_HEAVY;
 // 2 CTAs per SM) measured 4% faster than 2 targets per thread at 4 CTAs per SM (half the shared-memory reads per
 // pair, two independent lane groups per source).
 constexpr int kRtAdjoint = LDDMM_RT_ADJOINT;
-// The symmetric second-order forward step (pairs_kernel_sym): 4 targets per thread (8 would need more than the
-// 48 KiB of static shared memory for its compensated row sums; the per-step shuffles and loads that more targets
-// would amortise run beside the FMA pipe, which bounds the step).
+// The symmetric second-order forward step (pairs_kernel_sym): 8 targets per thread (168 registers, 3 CTAs per SM,
+// its compensated row sums in 48 KiB of dynamic shared memory) measured 15% faster at level 6 than 4 targets per
+// thread (134 registers, 3 CTAs per SM): the per-step source loads and the column shuffles are shared by twice
+// as many pairs, and four independent lane groups hide the latency of the ex2 chain.
 constexpr int kRtSymFwd = LDDMM_RT_SYM_FWD;
+// The symmetric K(x, x) a (pairs_kernel_symx): 8 targets per thread.
+constexpr int kRtKSym = LDDMM_RT_KSYM;
 // FP64 baseline path.
 constexpr int kTpb64 = LDDMM_TPB_64;
 constexpr int kRt64 = LDDMM_RT_64;

@@ -41,7 +41,10 @@
 #define LDDMM_SOBWD_SYM_MIN_CTAS 2  // the symmetric adjoint step (pairs_kernel_sym)
 #endif
 #ifndef LDDMM_SOFWD_SYM_MIN_CTAS
-#define LDDMM_SOFWD_SYM_MIN_CTAS 2  // the symmetric forward step (pairs_kernel_sym)
+#define LDDMM_SOFWD_SYM_MIN_CTAS 3  // the symmetric forward step (pairs_kernel_sym): caps it at 168 registers
+#endif
+#ifndef LDDMM_KSYM_MIN_CTAS
+#define LDDMM_KSYM_MIN_CTAS 4  // the symmetric K(x, x) a (pairs_kernel_symx): caps it at 128 registers
 #endif
 #ifndef LDDMM_FOBWD_MIN_CTAS
 #define LDDMM_FOBWD_MIN_CTAS 1
@@ -883,7 +886,7 @@ __global__ void finalize_kernel(const typename Op::Params P, int n, int tb_targe
 // Deterministic single-block sum of `count` doubles: out[0] = (accumulate ? out[0] : 0) + scale * sum(v).
 __global__ void ordered_sum_kernel(const double* __restrict__ v, int count, double scale, double* out, int accumulate);
 
-int resident_ctas(const void* kernel, int threads);
+int resident_ctas(const void* kernel, int threads, size_t dynamic_smem = 0);
 
 template <class Op, typename V, int TPB, int RT, class Fam = Gauss>
 inline int ctas_per_sm() {

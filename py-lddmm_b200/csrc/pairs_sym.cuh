@@ -39,8 +39,13 @@
 #ifndef LDDMM_SYM
 #define LDDMM_SYM 1  // 0: self-interaction sums evaluate every ordered pair (pairs_kernel)
 #endif
+#ifndef LDDMM_SYM_UNROLL
+#define LDDMM_SYM_UNROLL 4  // unroll depth of the 32-step source loop of a chunk (4: 1% faster than 2 at level 6)
+#endif
 
 namespace lddmm {
+
+constexpr int kSymUnroll = LDDMM_SYM_UNROLL;
 
 // first unit of row i (rows: target blocks; row i holds the tiles RT i .. TT - 1)
 __host__ __device__ __forceinline__ long long sym_row_off(long long i, long long TT, long long RT) {
@@ -96,7 +101,7 @@ __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymT
     float cs[Op::NC];
 #pragma unroll
     for (int c = 0; c < Op::NC; ++c) cs[c] = 0.f;
-#pragma unroll 2
+#pragma unroll kSymUnroll
     for (int s = 0; s < 32; ++s) {
       const int src = chunk * 32 + ((lane + s) & 31);
       F2 sv[2 * NU];
@@ -140,7 +145,10 @@ __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
   static_assert(TPB % 32 == 0 && RT % L == 0, "launch shape");
   __shared__ Unit<F2> sm[NU][TPB];
   __shared__ float colacc[NC][TPB];
-  __shared__ F2 cs[G * NR * 2][TPB];  // compensated row sums of the segment, one private column per thread
+  // compensated row sums of the segment, one private column per thread (G * NR * 2 rows of TPB): dynamic shared
+  // memory, so that 8 targets per thread may take more than the 48 KiB of static shared memory
+  extern __shared__ __align__(16) unsigned char sym_dyn_smem[];
+  F2 (*cs)[TPB] = reinterpret_cast<F2 (*)[TPB]>(sym_dyn_smem);
   const Frame& f = P.f;
 
   const long long u_end = sk_start(blockIdx.x + 1, U, C);
@@ -257,11 +265,40 @@ __global__ void finalize_sym_kernel(const typename Op::Params P, int n, int nblk
   Op::finalize_sym(P, idx, row, col);
 }
 
+// Dynamic shared memory of pairs_kernel_sym (its compensated row sums).
+template <class Op, int TPB, int RT>
+constexpr size_t sym_dyn_smem_bytes() {
+  return (size_t)(RT / 2) * Op::NR * 2 * TPB * sizeof(F2);
+}
+
+// Declare the kernel's dynamic shared memory, once per device (the attribute belongs to the device's context):
+// without it static + dynamic shared memory may not exceed 48 KiB. Returns false when the device refuses.
+template <class Op, int TPB, int RT>
+inline bool sym_prepare() {
+  static signed char state[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (dev < 0 || dev >= 64) return false;
+  if (state[dev] == 0) {
+    const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT>),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sym_dyn_smem_bytes<Op, TPB, RT>());
+    if (e != cudaSuccess) cudaGetLastError();
+    state[dev] = e == cudaSuccess ? 1 : -1;
+  }
+  return state[dev] > 0;
+}
+
 template <class Op, int TPB, int RT>
 inline int sym_ctas_per_sm() {
   static int cached = 0;
   if (cached == 0) {
-    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT>), TPB);
+    sym_prepare<Op, TPB, RT>();
+    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT>), TPB,
+                          sym_dyn_smem_bytes<Op, TPB, RT>());
     cached = c > 0 ? c : 2;
   }
   return cached;
@@ -279,10 +316,325 @@ inline int run_pairs_sym(const typename Op::Params& P, int64_t n, void* ws, size
   const SymPlan plan = make_sym_plan<TPB, RT>(n, Op::NR, Op::NC, sym_ctas_per_sm<Op, TPB, RT>());
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (ws == nullptr) return kInvalidArgument;
+  if (!sym_prepare<Op, TPB, RT>()) return kLaunchFailure;
   auto* row_ws = reinterpret_cast<float2*>(ws);
   auto* col_ws = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.col_off);
-  pairs_kernel_sym<Op, TPB, RT><<<plan.C, TPB, 0, stream>>>(P, (int)n, plan.nblk, plan.TT, plan.U, plan.C, row_ws,
-                                                            col_ws);
+  pairs_kernel_sym<Op, TPB, RT><<<plan.C, TPB, sym_dyn_smem_bytes<Op, TPB, RT>(), stream>>>(
+      P, (int)n, plan.nblk, plan.TT, plan.U, plan.C, row_ws, col_ws);
+  const int fb = 256;
+  finalize_sym_kernel<Op, TPB, RT><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT, plan.U,
+                                                                                 plan.C, row_ws, col_ws);
+  return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
+}
+
+
+// ---------------------------------------------------------------------------------------------------------
+// Expanded-distance form of the symmetric kernel, for sums whose pair term is the kernel value times a payload of
+// the source (K a over one point set: out_k = sum_l e_kl a_l, so the mirrored term of l is e_kl a_k).
+//
+// As in pairs_kernel_x, the coordinates of a unit are taken relative to the centre of its row block i (box centre
+// of the block's TPB * RT points, scaled): e_kl = f_k w_kl with f_k = 2^-|y_k|^2 and w_kl = 2^-(|x_l|^2 - 2 y_k.x_l),
+// the bracket being three packed FMAs from the staged fields (-2 x_l, |x_l|^2). The row sums of k accumulate
+// w_kl a_l and are multiplied by f_k (FP64) when the segment's partial is written; the column payload of target k is
+// f_k a_k, so the column sums accumulate w_kl f_k a_k = e_kl a_k directly. 9 FP32 lane-ops and one ex2 per
+// unordered pair (against 6 + 1 per ordered pair, i.e. 12 + 2, for pairs_kernel_x). Row blocks whose radius^2
+// (scaled units) exceeds kExpandR2 use the difference form (e from |y - x|^2, payload a_k; 12 + 1), chosen per
+// segment. Everything else -- the unit triangle, the rotating column accumulators, the stream-K split, the partial
+// layouts and finalize_sym_kernel -- is pairs_kernel_sym's.
+//
+// Op interface: Params, NP (payload fields; NR = NC = NP), kSymMinCtas, point(P, i, double* c) (coordinates of
+// point i), payload(P, i, double* p), finalize_sym(P, i, row, col).
+// ---------------------------------------------------------------------------------------------------------
+template <class Op, int TPB, int RT, bool COL, bool X>
+__device__ __forceinline__ void symx_tile(const F2 (&yt)[RT / 2][3], const F2 (&tp)[RT / 2][Op::NP],
+                                          const Unit<F2> (*sm)[TPB], float (*colacc)[TPB],
+                                          F2 (&acc)[RT / 2][Op::NP]) {
+  constexpr int G = RT / 2, NP = Op::NP, NU = (4 + NP + 1) / 2, W = TPB / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
+  for (int ph = 0; ph < W; ++ph) {
+    const int chunk = (warp + ph) % W;
+    float cs[NP];
+#pragma unroll
+    for (int c = 0; c < NP; ++c) cs[c] = 0.f;
+#pragma unroll kSymUnroll
+    for (int s = 0; s < 32; ++s) {
+      const int src = chunk * 32 + ((lane + s) & 31);
+      F2 sv[2 * NU];
+#pragma unroll
+      for (int q = 0; q < NU; ++q) {
+        const Unit<F2> w = sm[q][src];
+        sv[2 * q] = w.a;
+        sv[2 * q + 1] = w.b;
+      }
+      F2 col[NP];
+      if constexpr (COL) {
+#pragma unroll
+        for (int c = 0; c < NP; ++c) col[c] = f2(cs[c], 0.f);
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        F2 arg;
+        if constexpr (X) {
+          arg = fma(yt[g][2], sv[2], sv[3]);  // |x|^2 - 2 y.x
+          arg = fma(yt[g][1], sv[1], arg);
+          arg = fma(yt[g][0], sv[0], arg);
+        } else {
+          const F2 d0 = yt[g][0] - sv[0], d1 = yt[g][1] - sv[1], d2 = yt[g][2] - sv[2];
+          arg = fma(d2, d2, fma(d1, d1, d0 * d0));
+        }
+        const F2 e = VT<F2>::expneg(arg);
+#pragma unroll
+        for (int c = 0; c < NP; ++c) acc[g][c] = fma(e, sv[4 + c], acc[g][c]);
+        if constexpr (COL) {
+#pragma unroll
+          for (int c = 0; c < NP; ++c) col[c] = fma(e, tp[g][c], col[c]);
+        }
+      }
+      if constexpr (COL) {
+#pragma unroll
+        for (int c = 0; c < NP; ++c) {
+          float lo, hi;
+          split(col[c], lo, hi);
+          cs[c] = __shfl_sync(0xffffffffu, lo + hi, (lane + 1) & 31);
+        }
+      }
+    }
+    if constexpr (COL) {
+#pragma unroll
+      for (int c = 0; c < NP; ++c) colacc[c][chunk * 32 + lane] += cs[c];
+    }
+    __syncthreads();  // the next phase hands this chunk (and its column accumulators) to another warp
+  }
+}
+
+template <class Op, int TPB, int RT>
+__global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
+    pairs_kernel_symx(const typename Op::Params P, int n, int nblk, int TT, long long U, int C,
+                      float2* __restrict__ row_ws, float* __restrict__ col_ws) {
+  constexpr int L = 2, G = RT / L, NP = Op::NP, NU = (4 + NP + 1) / 2;
+  constexpr int B = TPB * RT;
+  static_assert(TPB % 32 == 0 && RT % L == 0, "launch shape");
+  __shared__ Unit<F2> sm[NU][TPB];
+  __shared__ float colacc[NP][TPB];
+  __shared__ float red[6][TPB / 32];
+  extern __shared__ __align__(16) unsigned char sym_dyn_smem[];
+  F2 (*cs)[TPB] = reinterpret_cast<F2 (*)[TPB]>(sym_dyn_smem);  // compensated row sums, G * NP * 2 rows
+  const Frame& f = P.f;
+  const double fo[3] = {f.o0, f.o1, f.o2};
+
+  const long long u_end = sk_start(blockIdx.x + 1, U, C);
+  long long u = sk_start(blockIdx.x, U, C);
+  int i = u < u_end ? sym_row_of(u, nblk, TT, RT) : 0;
+  while (u < u_end) {
+    const long long off = sym_row_off(i, TT, RT);
+    const int cnt = TT - RT * i;
+    const int t0 = (int)(u - off);
+    const int t1 = (int)((u_end - off) < cnt ? (u_end - off) : cnt);
+    const int slot = (int)blockIdx.x - sk_cta_of(off, U, C);
+    const int base = i * B + threadIdx.x;
+
+    // box and centre of row block i (every CTA working on it derives the same ones)
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+    for (int t = 0; t < RT; ++t) {
+      int k = base + t * TPB;
+      k = k < n ? k : n - 1;
+      double y[3];
+      Op::point(P, k, y);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float v = (float)((y[c] - fo[c]) * f.s);
+        lo[c] = fminf(lo[c], v);
+        hi[c] = fmaxf(hi[c], v);
+      }
+    }
+    block_box<TPB>(lo, hi, red);  // its barrier also orders the previous segment's last reads of sm and cs
+    float ob[3], rb2 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ob[c] = 0.5f * (lo[c] + hi[c]);
+      const float h = 0.5f * (hi[c] - lo[c]);
+      rb2 = fmaf(h, h, rb2);
+    }
+    const bool expand = rb2 <= kExpandR2;  // uniform over the CTA
+
+    F2 yt[G][3], tp[G][NP];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int k0 = base + (g * L) * TPB, k1 = base + (g * L + 1) * TPB;
+      double y0[3], y1[3], p0[NP], p1[NP];
+      Op::point(P, k0 < n ? k0 : n - 1, y0);
+      Op::point(P, k1 < n ? k1 : n - 1, y1);
+      Op::payload(P, k0 < n ? k0 : n - 1, p0);
+      Op::payload(P, k1 < n ? k1 : n - 1, p1);
+      double q0 = 0.0, q1 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float r0 = (float)((y0[c] - fo[c]) * f.s - (double)ob[c]);
+        const float r1 = (float)((y1[c] - fo[c]) * f.s - (double)ob[c]);
+        yt[g][c] = f2(r0, r1);
+        q0 += (double)r0 * (double)r0;
+        q1 += (double)r1 * (double)r1;
+      }
+      // column payload: f_k a_k (expanded form) or a_k; padded targets carry none
+      const double f0 = k0 < n ? (expand ? exp2(-q0) : 1.0) : 0.0;
+      const double f1 = k1 < n ? (expand ? exp2(-q1) : 1.0) : 0.0;
+#pragma unroll
+      for (int c = 0; c < NP; ++c) tp[g][c] = f2((float)(f0 * p0[c]), (float)(f1 * p1[c]));
+      Comp<F2> z;
+      z.zero();
+#pragma unroll
+      for (int c = 0; c < NP; ++c) z.template store<TPB>(cs, g * NP + c, threadIdx.x);
+    }
+
+    for (int tt = t0; tt < t1; ++tt) {
+      const int t = RT * i + tt;  // absolute source tile
+      const bool diag = tt < RT;  // tile of block i itself: rows only
+      {
+        const int l = t * TPB + threadIdx.x;
+        double fl[2 * NU];
+#pragma unroll
+        for (int q = 0; q < 2 * NU; ++q) fl[q] = 0.0;
+        if (l < n) {
+          double xr[3], r2 = 0.0;
+          Op::point(P, l, xr);
+          Op::payload(P, l, fl + 4);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const float xc = (float)((xr[c] - fo[c]) * f.s - (double)ob[c]);
+            r2 += (double)xc * (double)xc;
+            fl[c] = expand ? -2.0 * (double)xc : (double)xc;
+          }
+          fl[3] = r2;
+        }
+#pragma unroll
+        for (int q = 0; q < NU; ++q) {
+          Unit<F2> w;
+          w.a = VT<F2>::dup(fl[2 * q]);
+          w.b = VT<F2>::dup(fl[2 * q + 1]);
+          sm[q][threadIdx.x] = w;
+        }
+#pragma unroll
+        for (int c = 0; c < NP; ++c) colacc[c][threadIdx.x] = 0.f;
+      }
+      __syncthreads();
+      F2 acc[G][NP];
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int c = 0; c < NP; ++c) acc[g][c] = VT<F2>::zero();
+      if (expand) {
+        if (diag)
+          symx_tile<Op, TPB, RT, false, true>(yt, tp, sm, colacc, acc);
+        else
+          symx_tile<Op, TPB, RT, true, true>(yt, tp, sm, colacc, acc);
+      } else {
+        if (diag)
+          symx_tile<Op, TPB, RT, false, false>(yt, tp, sm, colacc, acc);
+        else
+          symx_tile<Op, TPB, RT, true, false>(yt, tp, sm, colacc, acc);
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int c = 0; c < NP; ++c) {
+          Comp<F2> m;
+          m.template load<TPB>(cs, g * NP + c, threadIdx.x);
+          m.merge(acc[g][c]);
+          m.template store<TPB>(cs, g * NP + c, threadIdx.x);
+        }
+      if (!diag) {
+        const int j = t / RT;
+        const size_t cb = (size_t)(sym_tri(j) + i) * NP * B + (size_t)(t - RT * j) * TPB + threadIdx.x;
+#pragma unroll
+        for (int c = 0; c < NP; ++c) col_ws[cb + (size_t)c * B] = colacc[c][threadIdx.x];
+      }
+      // the last phase barrier of symx_tile orders every read of sm and colacc before the next tile's staging
+    }
+
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        const int idx = base + (g * L + k) * TPB;
+        if (idx < n) {
+          double y2 = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double yr = VT<F2>::lane(yt[g][c], k);
+            y2 += yr * yr;
+          }
+          const double fac = expand ? exp2(-y2) : 1.0;
+#pragma unroll
+          for (int c = 0; c < NP; ++c) {
+            Comp<F2> m;
+            m.template load<TPB>(cs, g * NP + c, threadIdx.x);
+            const float2 pp = m.partial(k);
+            const double w = ((double)pp.x + (double)pp.y) * fac;
+            const float h = (float)w;
+            row_ws[((size_t)slot * NP + c) * (size_t)n + idx] = make_float2(h, (float)(w - (double)h));
+          }
+        }
+      }
+    u += t1 - t0;
+    ++i;
+  }
+}
+
+template <class Op, int TPB, int RT>
+constexpr size_t symx_dyn_smem_bytes() {
+  return (size_t)(RT / 2) * Op::NP * 2 * TPB * sizeof(F2);
+}
+
+template <class Op, int TPB, int RT>
+inline bool symx_prepare() {
+  static signed char state[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (dev < 0 || dev >= 64) return false;
+  if (state[dev] == 0) {
+    const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&pairs_kernel_symx<Op, TPB, RT>),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)symx_dyn_smem_bytes<Op, TPB, RT>());
+    if (e != cudaSuccess) cudaGetLastError();
+    state[dev] = e == cudaSuccess ? 1 : -1;
+  }
+  return state[dev] > 0;
+}
+
+template <class Op, int TPB, int RT>
+inline int symx_ctas_per_sm() {
+  static int cached = 0;
+  if (cached == 0) {
+    symx_prepare<Op, TPB, RT>();
+    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel_symx<Op, TPB, RT>), TPB,
+                          symx_dyn_smem_bytes<Op, TPB, RT>());
+    cached = c > 0 ? c : 2;
+  }
+  return cached;
+}
+
+template <class Op, int TPB, int RT>
+inline size_t symx_ws_bytes(int64_t n) {
+  return make_sym_plan<TPB, RT>(n, Op::NP, Op::NP, symx_ctas_per_sm<Op, TPB, RT>()).ws_bytes;
+}
+
+template <class Op, int TPB, int RT>
+inline int run_pairs_symx(const typename Op::Params& P, int64_t n, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  if (n <= 0) return kOk;
+  if (n > INT32_MAX / 4) return kInvalidArgument;
+  const SymPlan plan = make_sym_plan<TPB, RT>(n, Op::NP, Op::NP, symx_ctas_per_sm<Op, TPB, RT>());
+  if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
+  if (ws == nullptr) return kInvalidArgument;
+  if (!symx_prepare<Op, TPB, RT>()) return kLaunchFailure;
+  auto* row_ws = reinterpret_cast<float2*>(ws);
+  auto* col_ws = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.col_off);
+  pairs_kernel_symx<Op, TPB, RT><<<plan.C, TPB, symx_dyn_smem_bytes<Op, TPB, RT>(), stream>>>(
+      P, (int)n, plan.nblk, plan.TT, plan.U, plan.C, row_ws, col_ws);
   const int fb = 256;
   finalize_sym_kernel<Op, TPB, RT><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT, plan.U,
                                                                                  plan.C, row_ws, col_ws);

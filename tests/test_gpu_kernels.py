@@ -120,6 +120,25 @@ def test_ragged_and_edge_sizes(n, m):
         assert rel_err(K.applyDiffKT(x, p, a, firstVar=y), O.apply_diff_kt(y, x, p, a, 0.7)) < 2e-5
 
 
+@pytest.mark.parametrize('n', [1, 7, 1023, 1024, 1025, 2049, 5000])
+@pytest.mark.parametrize('spread', ['ball', 'wide'])
+def test_self_sum_ragged_sizes(n, spread):
+    """K(x, x) a with one point array as targets and sources runs the symmetric kernel (each unordered pair once,
+    credited to both points; 1,024 points per block): sizes below, at and above one and two blocks, points in a
+    small ball (expanded-distance form) or spread far in kernel widths (difference form for wide blocks), against
+    the oracle and against the ordered-pair kernel (the same sum through a distinct target array)."""
+    import oracle as O
+    rng = np.random.default_rng(n)
+    scale = 0.5 if spread == 'ball' else 6.0
+    x = rng.normal(size=(n, 3)) * scale
+    a = rng.normal(size=(n, 3))
+    K = kernel(0.7, 'float32')
+    out = K.applyK(x, a)
+    ref = O.apply_k(x, x, a, 0.7)
+    assert rel_err(out, ref) < 2e-5
+    assert rel_err(K.applyK(x, a, firstVar=x.copy()), ref) < 2e-5
+
+
 def test_full_size_properties_l6():
     """L6 (40,962 points): linearity, symmetry <b, K a> = <a, K b>, translation invariance and FP32 vs FP64."""
     import torch

@@ -143,3 +143,65 @@ def test_trained_proposal_beats_zero_momentum():
         it_warm = next((k for k, v in enumerate(warm.history) if v <= target * (1 + 1e-9)), len(warm.history))
         gains.append((it_plain, it_warm))
     assert sum(w for _, w in gains) < sum(p for p, _ in gains), gains
+
+
+def test_prolong_momentum_keeps_the_velocity_field():
+    """A smooth momentum on the level-3 sphere carried to the level-4 sphere generates the same velocity field at the
+    fine points (0.37% relative L2 in a float64 numpy emulation of the same formula; the bound leaves room for the
+    FP32 kernel sums)."""
+    import torch
+    from base import learnedProposal as lp
+    from base.kernelFunctions import Kernel
+    from base.syntheticShapes import icosphere
+    xc, Fc = icosphere(3)
+    xf, _ = icosphere(4)
+    rng = np.random.default_rng(0)
+    K = Kernel(name='gauss', sigma=0.5)
+    K.pk_dtype = 'float64'
+    Ks = Kernel(name='gauss', sigma=0.4)
+    Ks.pk_dtype = 'float64'
+    ac = Ks.applyK(xc, rng.normal(size=xc.shape))
+    af = lp.prolong_momentum(xc, ac, xf, K, 0.4 * lp.mean_edge_length(xc, Fc))
+    v_coarse = K.applyK(xc, ac, firstVar=xf)
+    v_fine = K.applyK(torch.from_numpy(xf).cuda(), af).cpu().numpy()
+    assert rel_err(v_fine, v_coarse) < 1e-2
+
+
+def test_multilevel_warm_start_reaches_the_plain_optimum_sooner():
+    """Coarse-to-fine warm start (network at the coarsest level, plain BFGS at levels 2 and 3, prolongation to level
+    4) on a bumpy-ellipsoid registration: the fine level takes the prolonged momentum, whose objective is far below
+    the zero-momentum start, and BFGS from it reaches the plain run's final objective in fewer fine iterations."""
+    import torch  # noqa: F401
+    from base import learnedProposal as lp
+    from base.kernelFunctions import Kernel
+    from base.surfaceMatching import SecondOrderSurfaceMatching
+    from base.surfaces import Surface
+    from base.syntheticShapes import icosphere, bumpy_ellipsoid
+    x0, F = icosphere(4)
+    x1 = bumpy_ellipsoid(x0, seed=3)
+    xs, Fs = icosphere(2)
+    feats, labels, _, n = lp.generate_pairs(xs, Fs, 128, seed=0, timeStep=0.1)
+    model = lp.MomentumProposal(seed=0)
+    lp.train(model, feats, labels, n, epochs=20, batch_pairs=16, lr=2e-3)
+
+    def matching(maxIter=60):
+        K = Kernel(name='gauss', sigma=0.5)
+        K.pk_dtype = 'float32'
+        opts = dict(maxIter=maxIter, affine='none', regWeight=1.0, KparDiff=K, KparDist=('gauss', 0.3),
+                    sigmaError=1.0, errorType='varifold', pk_dtype='float32', algorithm='bfgs', timeStep=0.1,
+                    verb=False)
+        return SecondOrderSurfaceMatching(Template=Surface(surf=(F, x0)), Target=Surface(surf=(F, x1)),
+                                          options=opts)
+
+    plain = matching()
+    obj_zero = plain.objectiveFun()
+    plain.optimizeMatching()
+    target = plain.history[-1]
+    warm = matching()
+    rec = lp.multilevel_warm_start(warm, model, [icosphere(2)[::-1], icosphere(3)[::-1]], rtol=1e-4)
+    assert [lv['vertices'] for lv in rec['levels']] == [162, 642]
+    assert rec['prolonged_used'] and rec['obj_prolonged'] < 0.2 * obj_zero, rec
+    warm.optimizeMatching()
+    it_plain = next(k for k, v in enumerate(plain.history) if v <= target * (1 + 1e-9))
+    it_warm = next((k for k, v in enumerate(warm.history) if v <= target * (1 + 1e-9)), len(warm.history))
+    assert it_warm < it_plain, (it_warm, it_plain)

@@ -256,6 +256,9 @@ def test_sharded_matching_nccl_single_rank():
     obj_u = fu.objectiveFun()
     g_u = fu.getGradient(1.0)['a0']
     fu.optimizeMatching()
-    assert abs(obj_s - obj_u) <= 1e-12 * abs(obj_u)
-    assert rel_err(g_s.cpu().numpy(), g_u.cpu().numpy()) < 1e-12
-    assert abs(fs.history[-1] - fu.history[-1]) <= 1e-10 * abs(fu.history[-1])
+    # At world size 1 the shooting and adjoint steps run the same (whole-step) kernels in both drivers; the kinetic
+    # term K(x0)a0 does not: the sharded driver sums its row range, the unsharded one evaluates the self-sum once per
+    # unordered pair. Both are FP32 compensated sums, so they agree to FP32 rounding, not bit for bit.
+    assert abs(obj_s - obj_u) <= 1e-9 * abs(obj_u)
+    assert rel_err(g_s.cpu().numpy(), g_u.cpu().numpy()) < 1e-6
+    assert abs(fs.history[-1] - fu.history[-1]) <= 1e-7 * abs(fu.history[-1])

@@ -86,7 +86,8 @@ def emulate(n, TPB, RT, wave, rng):
 
 
 @pytest.mark.parametrize('n,TPB,RT,wave', [(1, 128, 4, 296), (100, 128, 4, 296), (511, 32, 4, 7), (513, 32, 4, 7),
-                                           (2000, 32, 4, 13), (2000, 64, 2, 5), (1500, 32, 4, 1000), (777, 32, 6, 3)])
+                                           (2000, 32, 4, 13), (2000, 64, 2, 5), (1500, 32, 4, 1000), (777, 32, 6, 3),
+                                           (2100, 128, 8, 444), (3000, 32, 8, 17)])
 def test_symmetric_schedule_credits_every_pair_once(n, TPB, RT, wave):
     rng = np.random.default_rng(n + TPB + RT + wave)
     out, ref, credited = emulate(n, TPB, RT, wave, rng)
