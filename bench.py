@@ -60,13 +60,25 @@ sys.path.insert(0, REPO)
 
 LEVEL = 6
 SIGMAS = (0.25, 0.5)
-OPS_FP32_PER_PAIR = 6
-OPS_SFU_PER_PAIR = 1
+# The self-sum K(x,x)a runs the symmetric expanded-distance kernel (pairs_kernel_symx<OpKSym, 128, 8>): rows in
+# blocks of 128 x 8 points; an unordered pair of different blocks costs 9 FP32 lane-ops and one ex2 (row term,
+# column term, the expanded squared distance), an ordered pair inside a block 6 and one ex2 (row term only).
+KSYM_BLOCK = 1024
+OPS_FP32_OFFDIAG, OPS_FP32_DIAG, OPS_SFU_PER_PAIR = 9, 6, 1
 METRIC = 'Gauss kernel pairs/s'
-# Coarse-to-fine warm start of the registrations: the coarse levels (icosphere levels of the source) and the
-# relative objective decrease over 3 iterations below which a coarse level hands over to the next
-COARSE_LEVELS = (4, 5)
+# Coarse-to-fine warm start of the registrations: the coarse levels (icosphere levels of the source) per fine level,
+# and the relative objective decrease over 3 iterations below which a coarse level hands over to the next. At level
+# 6 one coarse level (4) measured faster than two (4, 5) on every seed tried: the level-5 stage costs more than the
+# fine iteration it saves.
+COARSE_LEVELS = {5: (3,), 6: (4,), 7: (4, 5)}
 COARSE_RTOL = 1e-4
+
+
+def coarse_templates(level, levels=None):
+    """Coarser triangulations (faces, vertices) of the level-`level` icosphere source, coarsest first."""
+    from base.syntheticShapes import icosphere
+    levels = COARSE_LEVELS.get(level, ()) if levels is None else levels
+    return [icosphere(lc)[::-1] for lc in levels if lc < level]
 # The reference's own numba applyK (ku.applyK_numba, float64) at N = M = 40,962: 22.2 s per call on 8 threads of an
 # Intel Xeon at 2.70 GHz, measured by importing the reference tree (which this benchmark does not read at run time).
 REFERENCE_NUMBA_APPLYK = {'value': 7.56e7, 'unit': 'pairs/s', 'cores': 8,
@@ -81,9 +93,20 @@ def workload():
     return x, a_raw
 
 
+def sym_pair_counts(n, block=KSYM_BLOCK):
+    """(ordered pairs evaluated inside row blocks, unordered pairs evaluated between blocks) of one symmetric K(x,x)a."""
+    nblk = (n + block - 1) // block
+    sizes = [block] * (nblk - 1) + [n - block * (nblk - 1)]
+    diag = sum(b * b for b in sizes)
+    return diag, (n * n - diag) // 2
+
+
 def config(n):
     return {'workload': 'L6 kernel sums: K(x,x)a, icosphere level 6, N=M=%d, sigma in %s, smoothed momenta' % (
         n, list(SIGMAS)), 'level': LEVEL, 'n_points': n, 'sigmas': list(SIGMAS), 'op': 'applyK (Gaussian)',
+        'pairs_counted': 'N(N+1)/2 per sum: the symmetric kernel evaluates each unordered pair once and credits '
+                         'both points (nm_equivalent_pairs_per_s counts the N*N ordered pairs of the same sums; '
+                         'the CPU baseline and the reference arm evaluate and count all N*N)',
         'arithmetic': 'FP32 pair sums with compensated (two-sum) accumulation, FP64 outputs',
         'l2': 'flushed between timed steps (256 MiB write)'}
 
@@ -409,15 +432,16 @@ def _fp64_energy(f):
     return float(f.objectiveFun())
 
 
-def train_proposal(pairs, heldout, epochs, seed=0):
-    """Network trained on pairs the method generates at level 4 (the last `heldout` pairs never trained on)."""
+def train_proposal(pairs, heldout, epochs, seed=0, law='noise'):
+    """Network trained on pairs the method generates at level 4 (the last `heldout` pairs never trained on);
+    `law`: the momentum law of the generated pairs (learnedProposal.generate_pairs)."""
     import torch
     from base import learnedProposal as lp
     from base.syntheticShapes import icosphere
     xs, Fs = icosphere(4)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    feats, labels, momenta, n4 = lp.generate_pairs(xs, Fs, pairs, seed=seed, timeStep=0.1)
+    feats, labels, momenta, n4 = lp.generate_pairs(xs, Fs, pairs, seed=seed, timeStep=0.1, law=law)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t0
     model = lp.MomentumProposal(seed=seed)
@@ -432,7 +456,8 @@ def train_proposal(pairs, heldout, epochs, seed=0):
         err = float((y - labels[ho, :n4]).norm() / labels[ho, :n4].norm())
     rec = {'level': 4, 'pairs': pairs, 'train_pairs': ntr, 'heldout_pairs': heldout, 'epochs': epochs,
            'generate_s': t_gen, 'train_s': t_train, 'loss_first_last': [hist[0], hist[-1]],
-           'heldout_label_rel_err': err, 'momentum_law': lp.MOMENTUM_LAW}
+           'heldout_label_rel_err': err,
+           'momentum_law': lp.MOMENTUM_LAW if law == 'noise' else lp.MOMENTUM_LAW_SHAPES}
     del feats, labels
     torch.cuda.empty_cache()
     return model, rec, (xs, Fs, momenta[ntr:])
@@ -502,6 +527,11 @@ def heldout_ellipsoids(model, seeds, level, coarse, tol=1e-3):
             else None}
 
 
+def _levels_arg(args):
+    v = getattr(args, 'coarse_levels', None)
+    return None if v in (None, '') else tuple(int(t) for t in v.split(',') if t.strip())
+
+
 def run_registration(args):
     """Seconds per registration pair to reach (E - E*)/E* <= 1e-3 on the level-6 icosphere -> bumpy ellipsoid problem
     (Gaussian sigma 0.5, varifold sigma 0.2, T = 20, sigmaError 1, BFGS): the plain FP64 path, the plain FP32 path,
@@ -514,10 +544,11 @@ def run_registration(args):
     x0, F = icosphere(level)
     x1 = bumpy_ellipsoid(x0, seed=0)
     sig, sigd, ts = 0.5, 0.2, 0.05
-    coarse = [icosphere(lc)[::-1] for lc in COARSE_LEVELS if lc < level]
+    levels = [lc for lc in (_levels_arg(args) or COARSE_LEVELS.get(level, ())) if lc < level]
+    coarse = coarse_templates(level, levels)
     res = {'problem': f'icosphere L{level} ({x0.shape[0]} vertices) -> bumpy ellipsoid (8 bumps), sigma {sig} / '
                       f'varifold {sigd}, T={int(round(1 / ts))}, sigmaError 1, BFGS', 'criterion': '(E - E*)/E* <= 1e-3',
-           'warm_start': {'coarse_levels': [lc for lc in COARSE_LEVELS if lc < level], 'coarse_rtol': COARSE_RTOL,
+           'warm_start': {'coarse_levels': levels, 'coarse_rtol': COARSE_RTOL,
                           'coarse_stop': 'relative objective decrease over 3 iterations below coarse_rtol',
                           'prolongation': 'momentum density interpolated by a normalised Gaussian of 0.4 x the '
                                           'coarse mean edge length'}}
@@ -600,6 +631,9 @@ def run_level4_fp64():
 OP_COUNTS = {'applyK': (6, 1), 'applyDiffKT_lddmm': (16, 1), 'applyDDiffK11and12': (23, 1), 'applyDiffK1and2': (16, 1),
              'so_step': (14, 1), 'so_adjoint_step': (37, 1), 'fo_adjoint_step': (19, 1), 'varifold_energy': (9, 1),
              'varifold_gradient': (19, 1)}
+# Self-sums that run a symmetric kernel (FP32, Gaussian): (row block size, FP32 lane-ops per ordered pair inside a
+# block (row terms only), FP32 lane-ops per unordered pair between blocks (row and column terms)); one ex2 each.
+SYM_COUNTS = {'applyK': (1024, 6, 9), 'so_step': (1024, 16, 22), 'so_adjoint_step': (512, 42, 51)}
 
 
 def mode_ops(args):
@@ -683,21 +717,39 @@ def mode_ops(args):
         pps = pairs[name] / (ms * 1e-3)
         fp32, sfu = OP_COUNTS[name]
         gauss = kern == nat.KERNEL_GAUSS or name.startswith('varifold')   # the op counts are the Gaussian ones
-        print(json.dumps({'op': name, 'kernel': args.kernel if not name.startswith('varifold') else 'gauss',
-                          'level': args.level, 'precision': args.precision, 'ms': round(ms, 4), 'pairs_per_s': pps,
-                          'frac_fp32_peak': pps * fp32 / peak32 if args.precision == 'fp32' and gauss else None,
-                          'frac_sfu_peak': pps * sfu / peaksfu if gauss else None}), flush=True)
+        rec = {'op': name, 'kernel': args.kernel if not name.startswith('varifold') else 'gauss', 'level': args.level,
+               'precision': args.precision, 'ms': round(ms, 4), 'pairs_per_s': pps,
+               'frac_fp32_peak': pps * fp32 / peak32 if args.precision == 'fp32' and gauss else None,
+               'frac_sfu_peak': pps * sfu / peaksfu if gauss else None}
+        if name in SYM_COUNTS and args.precision == 'fp32' and kern == nat.KERNEL_GAUSS:
+            blk, c_in, c_between = SYM_COUNTS[name]
+            diag, between = sym_pair_counts(n, blk)
+            rec.update({'kernel_form': 'symmetric', 'pairs_per_s': (diag + between) / (ms * 1e-3),
+                        'nm_equivalent_pairs_per_s': pps,
+                        'frac_fp32_peak': (c_in * diag + c_between * between) / (ms * 1e-3) / peak32,
+                        'frac_sfu_peak': (diag + between) / (ms * 1e-3) / peaksfu})
+        print(json.dumps(rec), flush=True)
 
 
 def mode_registration_profile(args):
-    """A few BFGS iterations of the level-6 registration (FP32 or FP64): wall time per iteration."""
+    """A few BFGS iterations of the level-6 registration (FP32 or FP64): wall time per iteration. With --warm
+    multilevel, the coarse-to-fine warm start (without the network) runs first and the fine level then makes --iters
+    iterations: the launch list of the registration path that the learned warm start takes."""
     from base.syntheticShapes import icosphere, bumpy_ellipsoid
     x0, F = icosphere(args.reg_level)
     x1 = bumpy_ellipsoid(x0, seed=0)
     dtype = 'float64' if args.precision == 'fp64' else 'float32'
-    f, _, s, _ = _register(x0, F, x1, dtype, 0.5, 0.2, 0.05, maxIter=args.iters)
-    print(json.dumps({'level': args.reg_level, 'dtype': dtype, 'iters': args.iters, 's': s,
-                      's_per_iter': s / args.iters, 'objective': f.history[-1]}), flush=True)
+    coarse = None
+    if args.warm == 'multilevel':
+        levels = [lc for lc in (_levels_arg(args) or COARSE_LEVELS.get(args.reg_level, ())) if lc < args.reg_level]
+        coarse = coarse_templates(args.reg_level, levels)
+    f, _, s, rec = _register(x0, F, x1, dtype, 0.5, 0.2, 0.05, maxIter=args.iters, coarse=coarse)
+    out = {'level': args.reg_level, 'dtype': dtype, 'iters': args.iters, 's': s, 's_per_iter': s / args.iters,
+           'objective': f.history[-1]}
+    if coarse is not None:
+        out['warm_start'] = {'coarse_iters': [lv['iters'] for lv in rec['levels']], 'prolonged_used':
+                             rec['prolonged_used']}
+    print(json.dumps(out), flush=True)
 
 
 def mode_large_registration(args):
@@ -705,7 +757,8 @@ def mode_large_registration(args):
       1. plain FP32 from zero momentum to the BFGS stopping rule; its final momentum re-evaluated on the FP64 path
          gives E*, and its first iterate within tolerance gives the plain FP32 iterations and seconds (a full FP64
          run to the stopping rule takes hours here, so E* comes from the FP32 run and is labelled so);
-      2. FP32 from the learned proposal (network trained at level 4, applied per vertex) to E* (1 + tol);
+      2. FP32 from the learned proposal (network trained at level 4, applied per vertex) to E* (1 + tol), and from
+         the coarse-to-fine warm start with and without the network (coarse levels 4 and 5 by default);
       3. the plain FP64 path timed over --fp64-probe-iters iterations; its time to tolerance is ESTIMATED as its
          first iteration plus (plain FP32 iterations to tolerance - 1) x its later seconds per iteration."""
     import torch
@@ -731,6 +784,16 @@ def mode_large_registration(args):
                            'obj_proposal': used[1], 'obj_zero': used[2], 'scale': used[3]}
     del fl
     torch.cuda.empty_cache()
+    levels = [lc for lc in (_levels_arg(args) or COARSE_LEVELS.get(7, ())) if lc < 7]
+    for name, model_ in (('multilevel_plain_fp32', None), ('learned_multilevel_fp32', model)):
+        fm, _, sm_, rec = _register(x0, F, x1, 'float32', sig, sigd, ts, target=target, model=model_,
+                                    coarse=coarse_templates(7, levels))
+        out[name] = {'fine_iters': len(fm.history), 's_to_tol': sm_, 'reached': bool(fm.reached_target),
+                     'rel_energy_fp64': (_fp64_energy(fm) - estar) / abs(estar), 'coarse_levels': levels,
+                     'coarse_iters': [lv['iters'] for lv in rec['levels']],
+                     'network_proposal_used': rec['network_proposal_used'], 'prolonged_used': rec['prolonged_used']}
+        del fm
+        torch.cuda.empty_cache()
     k = max(2, args.fp64_probe_iters)
     f64, t0, s64, _ = _register(x0, F, x1, 'float64', sig, sigd, ts, maxIter=k)
     first = f64.times[0] - t0
@@ -739,7 +802,9 @@ def mode_large_registration(args):
     if it32 is not None:
         est = first + per_it * (it32 - 1)
         out['plain_fp64_s_to_tol_ESTIMATE'] = est
-        out['speedup_learned_vs_plain_fp64_ESTIMATE'] = est / sl
+        out['speedup_learned_vs_plain_fp64_ESTIMATE'] = est / out['learned_multilevel_fp32']['s_to_tol']
+        out['speedup_learned_single_level_vs_plain_fp64_ESTIMATE'] = est / sl
+        out['speedup_multilevel_plain_vs_plain_fp64_ESTIMATE'] = est / out['multilevel_plain_fp32']['s_to_tol']
         out['speedup_plain_fp32_vs_plain_fp64_ESTIMATE'] = est / s32
     print(json.dumps(out), flush=True)
 
@@ -856,7 +921,8 @@ def run_b200(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t)
-    pairs_per_step = len(SIGMAS) * n * n
+    # pairs of the sum: each unordered pair {k, l} (and k = l) once, as the symmetric kernel evaluates them
+    pairs_per_step = len(SIGMAS) * n * (n + 1) // 2
     value = world * pairs_per_step * args.steps / (total_ms * 1e-3)
 
     # end-to-end through the reference-facing API (numpy in / numpy out)
@@ -894,8 +960,9 @@ def run_b200(args, rank, world, local_rank):
     peak_fp32 = n_sm * 128 * sm_max * 1e6 / 1e12          # T lane-ops/s
     peak_sfu = n_sm * 16 * sm_max * 1e6 / 1e12            # T ex2/s
     mean_launch_s = statistics.mean(launch_ms) * 1e-3
-    achieved = n * n * OPS_SFU_PER_PAIR / mean_launch_s / 1e12
-    fp32_frac = (n * n * OPS_FP32_PER_PAIR / mean_launch_s / 1e12) / peak_fp32
+    diag, off = sym_pair_counts(n)
+    achieved = (OPS_FP32_DIAG * diag + OPS_FP32_OFFDIAG * off) / mean_launch_s / 1e12      # T lane-ops/s
+    sfu_frac = (OPS_SFU_PER_PAIR * (diag + off) / mean_launch_s / 1e12) / peak_sfu
     traffic, traffic_source = ncu_traffic()
     cb_targets = args.cpu_targets
     import numba
@@ -908,13 +975,16 @@ def run_b200(args, rank, world, local_rank):
         'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': config(n),
         'e2e': {'value': e2e_value, 'unit': 'pairs/s', 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
                 'ms_per_step': float(te) / args.steps, 'api': 'Kernel.applyK(numpy x, numpy a)'},
-        'roofline': {'bound': 'sfu', 'achieved': achieved, 'peak': peak_sfu, 'unit': 'T ex2/s',
-                     'frac': achieved / peak_sfu, 'fp32_frac': fp32_frac, 'traffic': traffic,
+        'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak_fp32, 'unit': 'T FP32 lane-ops/s',
+                     'frac': achieved / peak_fp32, 'sfu_frac': sfu_frac, 'traffic': traffic,
                      'traffic_source': traffic_source, 'algorithmic_bytes': 2 * n * 3 * 8 + n * 3 * 8,
-                     'kernel': 'pairs_kernel_x<OpK, 128, 8> + finalize_kernel (timed together per call)',
-                     'ops_per_pair': {'fp32': OPS_FP32_PER_PAIR, 'sfu': OPS_SFU_PER_PAIR},
-                     'peak_source': f'{n_sm} SMs x 16 MUFU lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
-                                    f'max SM clock; MEASURED_PEAKS.json has no MUFU or FP32 figure)'},
+                     'kernel': 'pairs_kernel_symx<OpKSym, 128, 8> + finalize_sym_kernel (timed together per call)',
+                     'pairs_evaluated_per_launch': {'ordered_in_block': diag, 'unordered_between_blocks': off},
+                     'ops_per_pair': {'fp32_between_blocks': OPS_FP32_OFFDIAG, 'fp32_in_block': OPS_FP32_DIAG,
+                                      'sfu': OPS_SFU_PER_PAIR},
+                     'peak_source': f'{n_sm} SMs x 128 FP32 lanes x {sm_max:.0f} MHz (nominal pipe peak at the '
+                                    f'max SM clock; MEASURED_PEAKS.json has no FP32 figure)'},
+        'nm_equivalent_pairs_per_s': value * n / ((n + 1) / 2),
         'cpu_baseline': {'value': cb_val, 'unit': 'pairs/s', 'cores': cb_threads, 'kind': 'port',
                          'sample': f'{cb_pairs:.3g} pairs: blocks of {cb_targets} targets x {n} sources x '
                                    f'{len(SIGMAS)} widths, float64; port: the oracle numba restatement of '
@@ -949,6 +1019,7 @@ def main():
     ap.add_argument('--heldout-pairs', type=int, default=2000)
     ap.add_argument('--heldout-eval', type=int, default=8, help='held-out pairs registered with and without the net')
     ap.add_argument('--heldout-seeds', default='1,2', help='bumpy-ellipsoid seeds registered as held-out problems')
+    ap.add_argument('--coarse-levels', default='', help='coarse icosphere levels of the warm start (default: per level)')
     ap.add_argument('--train-epochs', type=int, default=4)
     # mode ops / registration-profile / large-registration
     ap.add_argument('--level', type=int, default=6)
@@ -959,6 +1030,7 @@ def main():
     ap.add_argument('--sigma-dist', type=float, default=0.2)
     ap.add_argument('--kernel', default='gauss', help="deformation kernel of --mode ops: 'gauss' or 'laplacian:<q>'")
     ap.add_argument('--iters', type=int, default=6)
+    ap.add_argument('--warm', default='none', choices=['none', 'multilevel'], help='mode registration-profile')
     ap.add_argument('--fp64-probe-iters', type=int, default=5)
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))

@@ -40,6 +40,14 @@ MOMENTUM_SCALE = 0.3
 # no registration produces), and its tangential part is invisible to the varifold data term (an ill-posed label).
 MOMENTUM_LAW = ('a = (K_0.4 z) n: a scalar white-noise field z smoothed at width 0.4, along the vertex normals n, '
                 'rescaled to a maximum initial speed drawn from U[0.05, 0.35]; shot with sigma 0.5, T = 10')
+# The 'shapes' law: normal fields of the kinds of deformation a surface registration meets -- a random quadratic
+# form (an ellipsoidal stretch: x^T M x with M a random symmetric matrix), a few Gaussian bumps (random centres on
+# the surface, widths U[0.15, 0.45], signed heights) and the smoothed noise of MOMENTUM_LAW -- mixed with random
+# weights and rescaled in speed like MOMENTUM_LAW.
+MOMENTUM_LAW_SHAPES = ('a = (w1 q + w2 b + w3 K_0.4 z) n: q = x^T M x (M symmetric, N(0,1) entries), b = sum of '
+                       'U{0..12} Gaussian bumps (centres on the surface, widths U[0.15, 0.45], heights N(0,1)), z '
+                       'white noise, weights U[0,1], each field scaled to max 1; rescaled to a maximum initial speed '
+                       'U[0.05, 0.35]; shot with sigma 0.5, T = 10')
 SCALAR_WIDTHS = (0.1, 0.2, 0.35, 0.7)
 ROW_PAD = 64
 
@@ -211,14 +219,43 @@ class MomentumProposal:
 # ---------------------------------------------------------------------------------------------------------------
 # Training data generated by the method itself, and training
 # ---------------------------------------------------------------------------------------------------------------
-def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, timeStep=0.1, vmin=0.05, vmax=0.35):
+def _shape_field(X0, gen, rng, Ksm):
+    """One scalar field of the 'shapes' law (N,1): the quadratic form, the bumps and the smoothed noise, each scaled
+    to max |.| = 1 and mixed with U[0,1] weights. Scalar parameters come from the host generator `rng` (no device
+    synchronisation), the noise from the device generator `gen`."""
+    n = X0.shape[0]
+    dev, f64 = X0.device, torch.float64
+    c = X0 - X0.mean(dim=0, keepdim=True)
+    M = rng.normal(size=(3, 3))
+    M = torch.from_numpy(0.5 * (M + M.T)).to(dev)
+    q = ((c @ M) * c).sum(dim=1, keepdim=True)
+    nb = int(rng.integers(0, 13))
+    b = torch.zeros((n, 1), dtype=f64, device=dev)
+    if nb:
+        centres = X0[torch.from_numpy(rng.integers(0, n, nb)).to(dev)]                    # (nb, 3)
+        w = torch.from_numpy(rng.uniform(0.15, 0.45, nb)).to(dev)
+        h = torch.from_numpy(rng.normal(size=nb)).to(dev)
+        d2 = ((X0[:, None, :] - centres[None, :, :]) ** 2).sum(dim=2)                    # (n, nb)
+        b = (h[None, :] * torch.exp(-d2 / (2 * w[None, :] ** 2))).sum(dim=1, keepdim=True)
+    z = torch.randn((n, 1), generator=gen, dtype=f64, device=dev).expand(n, 3).contiguous()
+    zs = Ksm.applyK(X0, z)[:, :1]
+    wts = rng.uniform(0.0, 1.0, 3)
+    out = torch.zeros((n, 1), dtype=f64, device=dev)
+    for wt, fld in zip(wts, (q, b, zs)):
+        out = out + float(wt) * fld / fld.abs().max().clamp_min(1e-300)
+    return out
+
+
+def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, timeStep=0.1, vmin=0.05, vmax=0.35,
+                   law='noise'):
     """Features (n_pairs, Mpad, IN_DIM) bf16, labels (n_pairs, Mpad, 3) f32 and momenta (n_pairs, n, 3) f64 of pairs
     (x0, shoot(x0, a_i)).
 
     a_i = (K_{sigma_smooth} z) n with z a scalar white-noise field, rescaled to an initial speed ~ U[vmin, vmax]
     (several widths: a sum of such fields, one per width, with random weights U[0, 1]);
     targets shot with K_{sigma_def} over round(1/timeStep) steps; labels are the momentum densities a_i * mass
-    (mass of K_{sigma_def}), over MOMENTUM_SCALE."""
+    (mass of K_{sigma_def}), over MOMENTUM_SCALE. law='shapes' draws the scalar field from the law of
+    MOMENTUM_LAW_SHAPES instead of smoothed noise alone."""
     X0 = nat.as_device(x0)
     faces_t = torch.from_numpy(np.ascontiguousarray(faces, dtype=np.int64)).cuda()
     n = X0.shape[0]
@@ -239,9 +276,14 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     momenta = torch.zeros((n_pairs, n, 3), dtype=torch.float64, device='cuda')
     origin = nat.centroid(X0)
     mass = kernel_mass(Kdef, X0)
+    if law not in ('noise', 'shapes'):
+        raise ValueError(f'unknown momentum law {law!r}')
+    rng = np.random.default_rng(seed)
     for i in range(n_pairs):
         a = torch.zeros_like(X0)
-        for k in Ksm:
+        if law == 'shapes':
+            a = _shape_field(X0, gen, rng, Ksm[0]) * normals
+        for k in (Ksm if law == 'noise' else ()):
             z = torch.randn((n, 1), generator=gen, dtype=torch.float64, device='cuda').expand(n, 3).contiguous()
             f = k.applyK(X0, z)[:, :1]
             wt = torch.rand((), generator=gen, dtype=torch.float64, device='cuda') if len(Ksm) > 1 else 1.0

@@ -83,7 +83,7 @@ size_t kernel_sums_ws_bytes(int64_t n, int64_t m, int precision) {
   upd(op_ws<OpDiffK1and2, kTpbLight, kRtLight>(n, m, precision));
   upd(op_ws<OpDiv, kTpbLight, kRtLight>(n, m, precision));
   upd(op_ws<OpKTensor, kTpbLight, kRtLight>(n, m, precision));
-  if (LDDMM_SYM && precision == kFP32Compensated && n == m) upd(symx_ws_bytes<OpKSym, kTpbLight, kRtKSym>(n));
+  if (LDDMM_SYM && precision == kFP32Compensated && n == m) upd(symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n));
   return b;
 }
 
@@ -102,7 +102,7 @@ int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, 
     OpK::Params P;
     P.f = make_frame(origin, sigma, kernel, true);
     P.y = y; P.x = x; P.a = a; P.out = out;
-    return run_pairs_symx<OpKSym, kTpbLight, kRtKSym>(P, n, ws, wsb, (cudaStream_t)stream);
+    return run_pairs_symx<OpKSym, kTpbKSym, kRtKSym>(P, n, ws, wsb, (cudaStream_t)stream);
   }
   return dispatch<OpK, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, (cudaStream_t)stream,
                                             [&](OpK::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });

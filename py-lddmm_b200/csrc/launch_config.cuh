@@ -20,6 +20,9 @@
 #ifndef LDDMM_RT_SYM_FWD
 #define LDDMM_RT_SYM_FWD 8
 #endif
+#ifndef LDDMM_TPB_KSYM
+#define LDDMM_TPB_KSYM 128
+#endif
 #ifndef LDDMM_RT_KSYM
 #define LDDMM_RT_KSYM 8
 #endif
@@ -48,6 +51,7 @@ constexpr int kRtAdjoint = LDDMM_RT_ADJOINT;
 // as many pairs, and four independent lane groups hide the latency of the ex2 chain.
 constexpr int kRtSymFwd = LDDMM_RT_SYM_FWD;
 // The symmetric K(x, x) a (pairs_kernel_symx): 8 targets per thread.
+constexpr int kTpbKSym = LDDMM_TPB_KSYM;
 constexpr int kRtKSym = LDDMM_RT_KSYM;
 // FP64 baseline path.
 constexpr int kTpb64 = LDDMM_TPB_64;

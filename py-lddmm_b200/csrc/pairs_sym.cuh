@@ -39,6 +39,13 @@
 #ifndef LDDMM_SYM
 #define LDDMM_SYM 1  // 0: self-interaction sums evaluate every ordered pair (pairs_kernel)
 #endif
+#ifndef LDDMM_SYM_COMPACT
+#define LDDMM_SYM_COMPACT 1  // 0: the symmetric kernels stage sources in pairs_kernel's duplicated layout (measured
+                             // 3-6% slower at level 6: twice the bytes per unshared load)
+#endif
+#ifndef LDDMM_SYMX_COL_SPLIT
+#define LDDMM_SYMX_COL_SPLIT 0  // 1: pairs_kernel_symx accumulates the column terms of even and odd lane groups apart
+#endif
 #ifndef LDDMM_SYM_UNROLL
 #define LDDMM_SYM_UNROLL 4  // unroll depth of the 32-step source loop of a chunk (4: 1% faster than 2 at level 6)
 #endif
@@ -46,6 +53,54 @@
 namespace lddmm {
 
 constexpr int kSymUnroll = LDDMM_SYM_UNROLL;
+
+// Shared-memory record of a staged source tile. In the symmetric kernels the 32 lanes of a warp read 32 different
+// sources at every step (no broadcast), so the record size is what the loads cost: compact records hold each field
+// once in FP32 (float4 groups) and the packed (f, f) operands are formed in registers; the duplicated layout of
+// pairs_kernel (Unit<F2>: one 16-byte load gives two packed operands) reads twice the bytes.
+template <int NF, int TPB>
+struct SymStage {
+#if LDDMM_SYM_COMPACT
+  static constexpr int NQ = (NF + 3) / 4;  // float4 groups
+  using T = float4;
+  static __device__ __forceinline__ void store(T (*sm)[TPB], int t, const double* fl) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      sm[q][t] = make_float4((float)fl[4 * q], (float)fl[4 * q + 1], (float)fl[4 * q + 2], (float)fl[4 * q + 3]);
+  }
+  static __device__ __forceinline__ void load(const T (*sm)[TPB], int src, F2* sv) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const float4 w = sm[q][src];
+      sv[4 * q] = f2(w.x, w.x);
+      sv[4 * q + 1] = f2(w.y, w.y);
+      sv[4 * q + 2] = f2(w.z, w.z);
+      sv[4 * q + 3] = f2(w.w, w.w);
+    }
+  }
+#else
+  static constexpr int NQ = (NF + 1) / 2;  // 16-byte units of two duplicated fields
+  using T = Unit<F2>;
+  static __device__ __forceinline__ void store(T (*sm)[TPB], int t, const double* fl) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      Unit<F2> w;
+      w.a = VT<F2>::dup(fl[2 * q]);
+      w.b = VT<F2>::dup(fl[2 * q + 1]);
+      sm[q][t] = w;
+    }
+  }
+  static __device__ __forceinline__ void load(const T (*sm)[TPB], int src, F2* sv) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const Unit<F2> w = sm[q][src];
+      sv[2 * q] = w.a;
+      sv[2 * q + 1] = w.b;
+    }
+  }
+#endif
+  static constexpr int kFields = 4 * ((NF + 3) / 4);  // size of the FP64 field buffer and of the operand array
+};
 
 // first unit of row i (rows: target blocks; row i holds the tiles RT i .. TT - 1)
 __host__ __device__ __forceinline__ long long sym_row_off(long long i, long long TT, long long RT) {
@@ -92,8 +147,10 @@ inline SymPlan make_sym_plan(int64_t n, int nr, int nc, int ctas_per_sm) {
 
 template <class Op, int TPB, int RT, bool COL>
 __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymTgt (&tgt)[RT / 2],
-                                         const Unit<F2> (*sm)[TPB], float (*colacc)[TPB], F2 (&acc)[RT / 2][Op::NR]) {
-  constexpr int G = RT / 2, NU = (Op::NSS + 1) / 2, W = TPB / 32;
+                                         const typename SymStage<Op::NSS, TPB>::T (*sm)[TPB], float (*colacc)[TPB],
+                                         F2 (&acc)[RT / 2][Op::NR]) {
+  using St = SymStage<Op::NSS, TPB>;
+  constexpr int G = RT / 2, W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll 1
   for (int ph = 0; ph < W; ++ph) {
@@ -104,13 +161,8 @@ __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymT
 #pragma unroll kSymUnroll
     for (int s = 0; s < 32; ++s) {
       const int src = chunk * 32 + ((lane + s) & 31);
-      F2 sv[2 * NU];
-#pragma unroll
-      for (int q = 0; q < NU; ++q) {
-        const Unit<F2> w = sm[q][src];
-        sv[2 * q] = w.a;
-        sv[2 * q + 1] = w.b;
-      }
+      F2 sv[St::kFields];
+      St::load(sm, src, sv);
       if constexpr (COL) {
         F2 col[Op::NC];
 #pragma unroll
@@ -140,10 +192,11 @@ template <class Op, int TPB, int RT>
 __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
     pairs_kernel_sym(const typename Op::Params P, int n, int nblk, int TT, long long U, int C,
                      float2* __restrict__ row_ws, float* __restrict__ col_ws) {
-  constexpr int L = 2, G = RT / L, NU = (Op::NSS + 1) / 2, NR = Op::NR, NC = Op::NC;
+  using St = SymStage<Op::NSS, TPB>;
+  constexpr int L = 2, G = RT / L, NR = Op::NR, NC = Op::NC;
   constexpr int B = TPB * RT;
   static_assert(TPB % 32 == 0 && RT % L == 0, "launch shape");
-  __shared__ Unit<F2> sm[NU][TPB];
+  __shared__ typename St::T sm[St::NQ][TPB];
   __shared__ float colacc[NC][TPB];
   // compensated row sums of the segment, one private column per thread (G * NR * 2 rows of TPB): dynamic shared
   // memory, so that 8 targets per thread may take more than the 48 KiB of static shared memory
@@ -178,17 +231,11 @@ __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
       const bool diag = tt < RT;  // tile of block i itself: rows only
       {
         const int l = t * TPB + threadIdx.x;
-        double fl[2 * NU];
+        double fl[St::kFields];
 #pragma unroll
-        for (int q = 0; q < 2 * NU; ++q) fl[q] = 0.0;
+        for (int q = 0; q < St::kFields; ++q) fl[q] = 0.0;
         if (l < n) Op::source_fields_sym(P, l, fl);
-#pragma unroll
-        for (int q = 0; q < NU; ++q) {
-          Unit<F2> w;
-          w.a = VT<F2>::dup(fl[2 * q]);
-          w.b = VT<F2>::dup(fl[2 * q + 1]);
-          sm[q][threadIdx.x] = w;
-        }
+        St::store(sm, threadIdx.x, fl);
 #pragma unroll
         for (int c = 0; c < NC; ++c) colacc[c][threadIdx.x] = 0.f;
       }
@@ -347,9 +394,10 @@ inline int run_pairs_sym(const typename Op::Params& P, int64_t n, void* ws, size
 // ---------------------------------------------------------------------------------------------------------
 template <class Op, int TPB, int RT, bool COL, bool X>
 __device__ __forceinline__ void symx_tile(const F2 (&yt)[RT / 2][3], const F2 (&tp)[RT / 2][Op::NP],
-                                          const Unit<F2> (*sm)[TPB], float (*colacc)[TPB],
-                                          F2 (&acc)[RT / 2][Op::NP]) {
-  constexpr int G = RT / 2, NP = Op::NP, NU = (4 + NP + 1) / 2, W = TPB / 32;
+                                          const typename SymStage<4 + Op::NP, TPB>::T (*sm)[TPB],
+                                          float (*colacc)[TPB], F2 (&acc)[RT / 2][Op::NP]) {
+  using St = SymStage<4 + Op::NP, TPB>;
+  constexpr int G = RT / 2, NP = Op::NP, W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll 1
   for (int ph = 0; ph < W; ++ph) {
@@ -360,17 +408,15 @@ __device__ __forceinline__ void symx_tile(const F2 (&yt)[RT / 2][3], const F2 (&
 #pragma unroll kSymUnroll
     for (int s = 0; s < 32; ++s) {
       const int src = chunk * 32 + ((lane + s) & 31);
-      F2 sv[2 * NU];
-#pragma unroll
-      for (int q = 0; q < NU; ++q) {
-        const Unit<F2> w = sm[q][src];
-        sv[2 * q] = w.a;
-        sv[2 * q + 1] = w.b;
-      }
-      F2 col[NP];
+      F2 sv[St::kFields];
+      St::load(sm, src, sv);
+      F2 col[NP], col2[NP];
       if constexpr (COL) {
 #pragma unroll
-        for (int c = 0; c < NP; ++c) col[c] = f2(cs[c], 0.f);
+        for (int c = 0; c < NP; ++c) {
+          col[c] = f2(cs[c], 0.f);
+          col2[c] = VT<F2>::zero();
+        }
       }
 #pragma unroll
       for (int g = 0; g < G; ++g) {
@@ -387,13 +433,19 @@ __device__ __forceinline__ void symx_tile(const F2 (&yt)[RT / 2][3], const F2 (&
 #pragma unroll
         for (int c = 0; c < NP; ++c) acc[g][c] = fma(e, sv[4 + c], acc[g][c]);
         if constexpr (COL) {
+          if (LDDMM_SYMX_COL_SPLIT != 0 && (g & 1)) {  // resolved at compile time (the loop is unrolled)
 #pragma unroll
-          for (int c = 0; c < NP; ++c) col[c] = fma(e, tp[g][c], col[c]);
+            for (int c = 0; c < NP; ++c) col2[c] = fma(e, tp[g][c], col2[c]);
+          } else {
+#pragma unroll
+            for (int c = 0; c < NP; ++c) col[c] = fma(e, tp[g][c], col[c]);
+          }
         }
       }
       if constexpr (COL) {
 #pragma unroll
         for (int c = 0; c < NP; ++c) {
+          if constexpr (LDDMM_SYMX_COL_SPLIT != 0) col[c] = col[c] + col2[c];
           float lo, hi;
           split(col[c], lo, hi);
           cs[c] = __shfl_sync(0xffffffffu, lo + hi, (lane + 1) & 31);
@@ -412,10 +464,11 @@ template <class Op, int TPB, int RT>
 __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
     pairs_kernel_symx(const typename Op::Params P, int n, int nblk, int TT, long long U, int C,
                       float2* __restrict__ row_ws, float* __restrict__ col_ws) {
-  constexpr int L = 2, G = RT / L, NP = Op::NP, NU = (4 + NP + 1) / 2;
+  using St = SymStage<4 + Op::NP, TPB>;
+  constexpr int L = 2, G = RT / L, NP = Op::NP;
   constexpr int B = TPB * RT;
   static_assert(TPB % 32 == 0 && RT % L == 0, "launch shape");
-  __shared__ Unit<F2> sm[NU][TPB];
+  __shared__ typename St::T sm[St::NQ][TPB];
   __shared__ float colacc[NP][TPB];
   __shared__ float red[6][TPB / 32];
   extern __shared__ __align__(16) unsigned char sym_dyn_smem[];
@@ -493,9 +546,9 @@ __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
       const bool diag = tt < RT;  // tile of block i itself: rows only
       {
         const int l = t * TPB + threadIdx.x;
-        double fl[2 * NU];
+        double fl[St::kFields];
 #pragma unroll
-        for (int q = 0; q < 2 * NU; ++q) fl[q] = 0.0;
+        for (int q = 0; q < St::kFields; ++q) fl[q] = 0.0;
         if (l < n) {
           double xr[3], r2 = 0.0;
           Op::point(P, l, xr);
@@ -508,13 +561,7 @@ __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
           }
           fl[3] = r2;
         }
-#pragma unroll
-        for (int q = 0; q < NU; ++q) {
-          Unit<F2> w;
-          w.a = VT<F2>::dup(fl[2 * q]);
-          w.b = VT<F2>::dup(fl[2 * q + 1]);
-          sm[q][threadIdx.x] = w;
-        }
+        St::store(sm, threadIdx.x, fl);
 #pragma unroll
         for (int c = 0; c < NP; ++c) colacc[c][threadIdx.x] = 0.f;
       }
