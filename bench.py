@@ -432,7 +432,7 @@ def _fp64_energy(f):
     return float(f.objectiveFun())
 
 
-def train_proposal(pairs, heldout, epochs, seed=0, law='noise'):
+def train_proposal(pairs, heldout, epochs, seed=0, law='shapes'):
     """Network trained on pairs the method generates at level 4 (the last `heldout` pairs never trained on);
     `law`: the momentum law of the generated pairs (learnedProposal.generate_pairs)."""
     import torch
@@ -566,7 +566,8 @@ def run_registration(args):
                          'timed': 'same run as E*, to its first iterate within tolerance'}
     del f64
     torch.cuda.empty_cache()
-    model, res['proposal'], heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
+    model, res['proposal'], heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs,
+                                                     law=args.momentum_law)
     runs = (('plain_fp32', None, None), ('learned_fp32', model, None), ('multilevel_plain_fp32', None, coarse),
             ('learned_multilevel_fp32', model, coarse))
     for name, model_, coarse_ in runs:
@@ -633,7 +634,8 @@ OP_COUNTS = {'applyK': (6, 1), 'applyDiffKT_lddmm': (16, 1), 'applyDDiffK11and12
              'varifold_gradient': (19, 1)}
 # Self-sums that run a symmetric kernel (FP32, Gaussian): (row block size, FP32 lane-ops per ordered pair inside a
 # block (row terms only), FP32 lane-ops per unordered pair between blocks (row and column terms)); one ex2 each.
-SYM_COUNTS = {'applyK': (1024, 6, 9), 'so_step': (1024, 16, 22), 'so_adjoint_step': (512, 42, 51)}
+SYM_COUNTS = {'applyK': (1024, 6, 9), 'so_step': (1024, 16, 22), 'so_adjoint_step': (512, 42, 51),
+              'fo_adjoint_step': (512, 19, 25)}
 
 
 def mode_ops(args):
@@ -777,7 +779,8 @@ def mode_large_registration(args):
                          'estar_fp64_of_fp32_optimum': estar, 'iters_to_tol': it32, 's_to_tol': s32}
     del f32
     torch.cuda.empty_cache()
-    model, out['proposal'], _ = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
+    model, out['proposal'], _ = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs,
+                                               law=args.momentum_law)
     fl, _, sl, used = _register(x0, F, x1, 'float32', sig, sigd, ts, target=target, model=model)
     out['learned_fp32'] = {'iters': len(fl.history), 's_to_tol': sl, 'reached': bool(fl.reached_target),
                            'rel_energy_fp64': (_fp64_energy(fl) - estar) / abs(estar), 'proposal_used': used[0],
@@ -854,7 +857,8 @@ def mode_sharded_registration(args, rank, world, local_rank):
 
 def mode_proposal_eval(args):
     """Held-out evaluation of the learned proposal on level-4 shot pairs: iterations and seconds to tolerance."""
-    model, rec, heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs)
+    model, rec, heldset = train_proposal(args.train_pairs, args.heldout_pairs, args.train_epochs,
+                                                    law=args.momentum_law)
     rec['heldout_eval'] = heldout_registrations(model, heldset, args.heldout_eval)
     print(json.dumps(rec), flush=True)
 
@@ -1020,6 +1024,8 @@ def main():
     ap.add_argument('--heldout-eval', type=int, default=8, help='held-out pairs registered with and without the net')
     ap.add_argument('--heldout-seeds', default='1,2', help='bumpy-ellipsoid seeds registered as held-out problems')
     ap.add_argument('--coarse-levels', default='', help='coarse icosphere levels of the warm start (default: per level)')
+    ap.add_argument('--momentum-law', default='shapes', choices=['shapes', 'noise'],
+                    help='momentum law of the generated training pairs (learnedProposal.generate_pairs)')
     ap.add_argument('--train-epochs', type=int, default=4)
     # mode ops / registration-profile / large-registration
     ap.add_argument('--level', type=int, default=6)

@@ -240,6 +240,17 @@ int lddmm_adam_step(float* param, const float* grad, float* m1, float* m2, void*
 int lddmm_nearest_displacement(const double* src, int64_t n, const double* tgt, int64_t m, double* disp,
                                lddmm_stream_t stream);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * Optimiser: the L-BFGS search direction (replaces the two-loop recursion of base/bfgs.py:183-198).
+ * q(n) = H g for the m stored pairs (s_k, y_k), k = 0 oldest .. m-1 newest: rho_k = 1/(y_k.s_k), the initial
+ * scaling (s_{m-1}.y_{m-1})/(y_{m-1}.y_{m-1}) (1 when below 1e-10), all in FP64 and in one launch (one CTA, fixed
+ * reduction order). s and y are HOST arrays of m device pointers to n doubles each; g and q are device arrays of n
+ * doubles (q may not alias g, s or y). 1 <= m <= LDDMM_LBFGS_MAX_PAIRS. Meant for the small and medium controls
+ * of the coarse levels (n up to ~1e5), where the recursion from the host costs more than the shooting. */
+#define LDDMM_LBFGS_MAX_PAIRS 64
+int lddmm_lbfgs_direction(const double* const* s, const double* const* y, int m, const double* g, int64_t n,
+                          double* q, lddmm_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,7 +64,9 @@ SIGNATURES = {
     'lddmm_adam_step': [_dp, _dp, _dp, _dp, _dp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                         ctypes.c_float, _i64, ctypes.c_float, _vp],
     'lddmm_nearest_displacement': [_dp, _i64, _dp, _i64, _dp, _vp],
+    'lddmm_lbfgs_direction': [_vp, _vp, _int, _dp, _i64, _dp, _vp],
 }
+LBFGS_MAX_PAIRS = 64        # LDDMM_LBFGS_MAX_PAIRS of the header
 _RESTYPES = {'lddmm_version': ctypes.c_char_p, 'lddmm_status_string': ctypes.c_char_p,
              'lddmm_workspace_bytes': ctypes.c_size_t, 'lddmm_surface_workspace_bytes': ctypes.c_size_t}
 

@@ -32,6 +32,8 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
     dot = getattr(opt, 'dotProduct_euclidean', None) or getattr(opt, 'dotProduct', None) or _dot
     # optional: (u, v) -> u.v as a device scalar, used by the two-loop recursion (no host synchronisation)
     dot_dev = getattr(opt, 'dotProduct_device', None)
+    # optional: (gradient, history) -> the two-loop recursion's direction in one call, or None to run it here
+    fused_direction = getattr(opt, 'lbfgs_direction', None)
     addProd = getattr(opt, 'addProd', lambda x, y, a: x + a * y)
     prod = getattr(opt, 'prod', lambda x, a: a * x)
     copyDir = getattr(opt, 'copyDir', deepcopy)
@@ -91,30 +93,34 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
             logging.info(f'gradient check along a random direction: finite difference {(o1 - o2) / (2 * epsfoo):.4f}, '
                          f'analytic {-gd * gradCoeff:.4f}')
 
+        q = None
         if not opt.reset and it > 0:
             history.append([diffVar, addProd(grd, grdOld, -1)])
             if len(history) > memory:
                 history.pop(0)
-            q = copyDir(grd)
-            # the two-loop recursion; with `dot_dev` (device scalars) it runs without reading anything back
-            d = dot_dev or (lambda u, v: dot(u, [v])[0])
-            rho, alpha = [], []
-            for s_k, y_k in reversed(history):
-                rho.append(1 / d(y_k, s_k))
-                alpha.append(rho[-1] * d(s_k, q))
-                q = addProd(q, y_k, -alpha[-1])
-            rho.reverse()
-            alpha.reverse()
-            s_k, y_k = history[-1]
-            c = d(s_k, y_k) / d(y_k, y_k)
-            if dot_dev is not None:
-                c = torch.where(c < 1e-10, torch.ones_like(c), c)
-            elif c < 1e-10:
-                c = 1
-            q = prod(q, c)
-            for k, (s_k, y_k) in enumerate(history):
-                beta = rho[k] * d(y_k, q)
-                q = addProd(q, s_k, alpha[k] - beta)
+            if fused_direction is not None:
+                q = fused_direction(grd, history)
+            if q is None:
+                q = copyDir(grd)
+                # the two-loop recursion; with `dot_dev` (device scalars) it runs without reading anything back
+                d = dot_dev or (lambda u, v: dot(u, [v])[0])
+                rho, alpha = [], []
+                for s_k, y_k in reversed(history):
+                    rho.append(1 / d(y_k, s_k))
+                    alpha.append(rho[-1] * d(s_k, q))
+                    q = addProd(q, y_k, -alpha[-1])
+                rho.reverse()
+                alpha.reverse()
+                s_k, y_k = history[-1]
+                c = d(s_k, y_k) / d(y_k, y_k)
+                if dot_dev is not None:
+                    c = torch.where(c < 1e-10, torch.ones_like(c), c)
+                elif c < 1e-10:
+                    c = 1
+                q = prod(q, c)
+                for k, (s_k, y_k) in enumerate(history):
+                    beta = rho[k] * d(y_k, q)
+                    q = addProd(q, s_k, alpha[k] - beta)
         else:
             history = []
             q = copyDir(grd)

@@ -19,9 +19,14 @@ features give the network) rather than the velocity K a0 matters: started from t
 into a momentum by the normalised kernel inverse, BFGS needs as many iterations as from the network's velocity,
 three times more than from the exact momentum.
 
-Training data: pairs generated by the method itself -- random smooth normal momentum fields a = (K_s z) n (z a
-scalar white-noise field, rescaled to an initial speed drawn in [vmin, vmax]) shot with the deformation kernel; the
-label is the momentum density of the generating momentum.
+Training data: pairs generated by the method itself -- random smooth normal momentum fields shot with the
+deformation kernel; the label is the momentum density of the generating momentum. Two laws for the scalar field
+along the normals: 'noise' (a white-noise field smoothed by K_s, MOMENTUM_LAW) and 'shapes' (a mixture of a random
+quadratic form, Gaussian bumps and the smoothed noise, MOMENTUM_LAW_SHAPES: the kinds of deformation a surface
+registration meets); each is rescaled to an initial speed drawn in [vmin, vmax].
+
+Coarse to fine (multilevel_warm_start): the proposal is made on a coarse triangulation of the source, refined there
+by the plain optimiser, and its momentum density carried to the full-resolution source (prolong_momentum).
 """
 import math
 

@@ -16,6 +16,7 @@ Differences from the reference, by design:
   * affine parts, landmarks, symmetric / unreduced / SGD variants are not implemented; of the file output, the
     result record of `saveHdf5` is written as an .npz archive with the same keys (h5py is not available).
 """
+import ctypes
 import logging
 import time
 from copy import deepcopy
@@ -212,6 +213,37 @@ class _DeviceMatching:
             t = torch.dot(v.reshape(-1), g2[k].reshape(-1))
             tot = t if tot is None else tot + t
         return tot if tot is not None else torch.zeros((), dtype=torch.float64, device=self.x0.device)
+
+    # Controls of at most this many doubles take the L-BFGS direction from one library call (one CTA runs the whole
+    # two-loop recursion; at the coarse levels of a warm start the recursion from the host -- ~4 small kernels and
+    # Python calls per stored pair -- costs more than the shooting); larger ones run it from the host, whose kernels
+    # spread over the GPU.
+    LBFGS_FUSED_MAX = 1 << 16
+
+    def lbfgs_direction(self, grd, history):
+        """The optimiser's two-loop recursion (base/bfgs.py:183-198) for gradient `grd` and the stored pairs
+        `history` ([s_k, y_k], oldest first) in one call of lddmm_lbfgs_direction, or None when the controls do not
+        fit it (the optimiser then runs the recursion itself)."""
+        k = self.control_key
+        g = grd.get(k)
+        m = len(history)
+        if g is None or m < 1 or m > nat.LBFGS_MAX_PAIRS or g.numel() > self.LBFGS_FUSED_MAX:
+            return None
+        if any(v is not None for kk, v in grd.items() if kk != k):
+            return None
+        S = [h[0].get(k) for h in history]
+        Y = [h[1].get(k) for h in history]
+        for t in S + Y:
+            if t is None or t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.numel() != g.numel():
+                return None
+        g = g.contiguous()
+        q = torch.empty_like(g)
+        sp = (ctypes.c_void_p * m)(*[t.data_ptr() for t in S])
+        yp = (ctypes.c_void_p * m)(*[t.data_ptr() for t in Y])
+        nat.check(nat.lib().lddmm_lbfgs_direction(ctypes.cast(sp, ctypes.c_void_p), ctypes.cast(yp, ctypes.c_void_p),
+                                                  m, nat.ptr(g), g.numel(), nat.ptr(q), nat.stream_ptr()),
+                  'lbfgs_direction')
+        return Control({k: q})
 
     def dotProduct_euclidean(self, g1, g2):
         vals = [self.dotProduct_device(g1, gr) for gr in g2]

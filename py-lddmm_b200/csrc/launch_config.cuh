@@ -20,6 +20,9 @@
 #ifndef LDDMM_RT_SYM_FWD
 #define LDDMM_RT_SYM_FWD 8
 #endif
+#ifndef LDDMM_RT_FO_SYM
+#define LDDMM_RT_FO_SYM 4
+#endif
 #ifndef LDDMM_TPB_KSYM
 #define LDDMM_TPB_KSYM 128
 #endif
@@ -51,6 +54,8 @@ constexpr int kRtAdjoint = LDDMM_RT_ADJOINT;
 // as many pairs, and four independent lane groups hide the latency of the ex2 chain.
 constexpr int kRtSymFwd = LDDMM_RT_SYM_FWD;
 // The symmetric K(x, x) a (pairs_kernel_symx): 8 targets per thread.
+// The symmetric first-order adjoint step (pairs_kernel_sym): 4 targets per thread.
+constexpr int kRtFoSym = LDDMM_RT_FO_SYM;
 constexpr int kTpbKSym = LDDMM_TPB_KSYM;
 constexpr int kRtKSym = LDDMM_RT_KSYM;
 // FP64 baseline path.

@@ -47,6 +47,9 @@
 #define LDDMM_KSYM_MIN_CTAS 3  // the symmetric K(x, x) a (pairs_kernel_symx): 164 registers, 3 CTAs per SM (3% faster
                                // than 4 CTAs at 128 registers, which spill)
 #endif
+#ifndef LDDMM_FOBWD_SYM_MIN_CTAS
+#define LDDMM_FOBWD_SYM_MIN_CTAS 2  // the symmetric first-order adjoint step (pairs_kernel_sym)
+#endif
 #ifndef LDDMM_FOBWD_MIN_CTAS
 #define LDDMM_FOBWD_MIN_CTAS 1
 #endif

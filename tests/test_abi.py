@@ -49,6 +49,9 @@ def test_host_only_entry_points():
     assert lib.lddmm_apply_diff_kt(null, 4, null, null, null, 5, 0.5, 0, 2, 1.0, None, null, 0, null, 0, null) == 1
     assert lib.lddmm_second_order_shoot(null, null, 0, 1, 0.5, 3, 0.1, None, null, null, 0, null, 0, null) == 1
     assert lib.lddmm_workspace_bytes(10, 10, 7) == 0
+    # the L-BFGS direction takes 1..64 stored pairs
+    assert lib.lddmm_lbfgs_direction(null, null, 0, null, 10, null, null) == 1
+    assert lib.lddmm_lbfgs_direction(null, null, 65, null, 10, null, null) == 1
 
 
 def test_vertex_face_table_host():

@@ -205,3 +205,30 @@ def test_multilevel_warm_start_reaches_the_plain_optimum_sooner():
     it_plain = next(k for k, v in enumerate(plain.history) if v <= target * (1 + 1e-9))
     it_warm = next((k for k, v in enumerate(warm.history) if v <= target * (1 + 1e-9)), len(warm.history))
     assert it_warm < it_plain, (it_warm, it_plain)
+
+
+def test_shapes_law_pairs():
+    """The 'shapes' momentum law (quadratic stretch + bumps + smoothed noise along the normals): momenta are normal
+    fields, their initial speeds lie in [vmin, vmax], the labels are the momentum densities, and the draw is
+    reproducible from the seed (to rounding)."""
+    import torch
+    from base import learnedProposal as lp
+    from base.kernelFunctions import Kernel
+    from base.syntheticShapes import icosphere
+    x0, F = icosphere(3)
+    feats, labels, momenta, n = lp.generate_pairs(x0, F, 8, seed=5, timeStep=0.1, law='shapes', vmin=0.1, vmax=0.3)
+    X0 = torch.from_numpy(x0).cuda()
+    nrm = lp.vertex_normals(X0, torch.from_numpy(F).cuda())
+    K = Kernel(name='gauss', sigma=0.5)
+    K.pk_dtype = 'float64'
+    mass = lp.kernel_mass(K, X0)
+    for i in range(8):
+        a = momenta[i]
+        tangential = a - (a * nrm).sum(dim=1, keepdim=True) * nrm
+        assert float(tangential.norm()) < 1e-9 * float(a.norm())
+        v = K.applyK(X0, a).norm(dim=1).max()
+        assert 0.1 * (1 - 1e-5) <= float(v) <= 0.3 * (1 + 1e-5)   # speeds set with the FP32 kernel sum
+        assert rel_err(labels[i, :n].double().cpu().numpy(), (a * mass / lp.MOMENTUM_SCALE).cpu().numpy()) < 1e-6
+    # the vertex normals are accumulated with atomic adds (index_add_), so a second draw agrees to rounding
+    _, _, again, _ = lp.generate_pairs(x0, F, 8, seed=5, timeStep=0.1, law='shapes', vmin=0.1, vmax=0.3)
+    assert rel_err(again.cpu().numpy(), momenta.cpu().numpy()) < 1e-12

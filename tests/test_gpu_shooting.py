@@ -131,6 +131,36 @@ def test_first_order_energy_and_euclidean_gradient():
         assert rel_err(dat[t].cpu().numpy(), O.apply_k(d['xt'][t], d['xt'][t], g, 0.5)) < 1e-11
 
 
+def test_first_order_symmetric_kernels_level4():
+    """First-order shooting and adjoint at level 4 (2,562 points: several row blocks, so the FP32 symmetric kernels
+    credit pairs to both points), FP32 against the oracle: the trajectory, the kinetic energy, the covectors and the
+    euclidean gradient (relative L2 2e-5, the FP32 shooting tolerance)."""
+    import torch
+    import oracle as O
+    from base import pointEvolution as evol
+    from base.syntheticShapes import icosphere
+    x0, _ = icosphere(4)
+    rng = np.random.default_rng(21)
+    T, w = 5, 0.8
+    at = np.stack([O.apply_k(x0, x0, rng.normal(0, 0.02, x0.shape), 0.3) for _ in range(T)])
+    px1 = rng.normal(size=x0.shape)
+    K = kernel(0.5, 'float32')
+    e = torch.zeros(1, dtype=torch.float64, device='cuda')
+    AT = torch.from_numpy(at).cuda()
+    xt = evol.shoot_first_order(torch.from_numpy(x0).cuda(), AT, K, regweight=w, energy=e)
+    dat_ref, xt_ref, pxt_ref = O.landmark_hamiltonian_gradient(x0, at, px1, 0.5, w)
+    assert rel_err(xt.cpu().numpy() - x0, xt_ref - x0) < 2e-5
+    e_ref = sum(w / T * (at[t] * O.apply_k(xt_ref[t], xt_ref[t], at[t], 0.5)).sum() for t in range(T))
+    assert abs(float(e) - e_ref) < 2e-5 * abs(e_ref)
+    pxt, dat = evol.first_order_gradient(xt, AT, torch.from_numpy(px1).cuda(), K, w)
+    assert rel_err(pxt.cpu().numpy() - px1, pxt_ref - px1) < 2e-5
+    assert rel_err(dat.cpu().numpy(), dat_ref) < 2e-5
+    _, dat_e = evol.first_order_gradient(xt, AT, torch.from_numpy(px1).cuda(), K, w, euclidean=True)
+    for t in range(T):
+        g = 2 * w * at[t] - pxt_ref[t + 1]
+        assert rel_err(dat_e[t].cpu().numpy(), O.apply_k(xt_ref[t], xt_ref[t], g, 0.5)) < 2e-5
+
+
 @pytest.mark.parametrize('dtype', ['float32', 'float64'])
 def test_row_range_steps_match_whole_steps(dtype):
     """lddmm_second_order_step_rows / _adjoint_step_rows on a row range equal the same rows of the whole step."""
