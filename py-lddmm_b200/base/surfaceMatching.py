@@ -395,19 +395,31 @@ class SecondOrderSurfaceMatching(_DeviceMatching):
 
     def initialize_variables(self):
         a0 = self.options['initialMomentum']
+        self._zero_start = None
         if a0 is None:
+            # zero momentum: the geodesic stays at x0 with zero momentum (what shooting it gives, exactly), so the
+            # trajectory is written instead of shot; objectiveFunDef recognises this control by identity
             self.control['a0'] = torch.zeros((self.npt, 3), dtype=torch.float64, device=self.x0.device)
+            T = int(np.round(1.0 / self.options['timeStep']))
+            xt = self.x0.unsqueeze(0).repeat(T + 1, 1, 1)
+            at = torch.zeros((T + 1, self.npt, 3), dtype=torch.float64, device=self.x0.device)
+            self._zero_start = (self.control['a0'], State(xt=xt, at=at))
         else:
             self.control['a0'] = nat.as_device(a0).clone()
+            xt, at = evol.shoot_second_order(self.x0, self.control['a0'], self.options['KparDiff'],
+                                             self.options['timeStep'], origin=self.origin)
         self.control['Afft'] = None
-        xt, at = evol.shoot_second_order(self.x0, self.control['a0'], self.options['KparDiff'],
-                                         self.options['timeStep'], origin=self.origin)
         self.state = State(xt=xt, at=at)
 
     def objectiveFunDef(self, control, var=None, withTrajectory=True, withJacobian=False):
         """0.5 a0.K(x0)a0 with the geodesic trajectory (base/secondOrderPointSetMatching.py:113-148)."""
         K = self.options['KparDiff']
         a0 = control['a0']
+        zs = getattr(self, '_zero_start', None)
+        if zs is not None and a0 is zs[0]:
+            # the untouched zero start: kinetic energy 0 and the constant trajectory
+            obj = torch.zeros((), dtype=torch.float64, device=self.x0.device)
+            return (obj, zs[1]) if withTrajectory or withJacobian else obj
         sh = self._sharding()
         if sh is not None:
             dd, group, step_rows, _, k_rows, gather = sh
