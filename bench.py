@@ -863,6 +863,37 @@ def mode_proposal_eval(args):
     print(json.dumps(rec), flush=True)
 
 
+def ordered_pair_kernel(X, A, lib, nat, ws, wsb, o, sp, flush, peak_fp32, peak_sfu, warmup, reps=20):
+    """The same sums through the ordered-pair kernel (pairs_kernel_x<OpK, 128, 8>, the path of K(y,x)a with distinct
+    target and source arrays): a copy of x as the targets. Mean device time per sum (CUDA events, L2 flushed before
+    each), pairs/s over N^2 and its MUFU / FP32 fractions (6 lane-ops and one ex2 per ordered pair)."""
+    import torch
+    n = X.shape[0]
+    Y = X.clone()
+    out = torch.empty_like(X)
+    stream = torch.cuda.current_stream()
+    ms = []
+    for it in range(warmup + reps):
+        for s in SIGMAS:
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.lddmm_apply_k(nat.ptr(Y), n, nat.ptr(X), nat.ptr(A), n, s, nat.KERNEL_GAUSS, o, nat.ptr(out),
+                                   nat.FP32C, ws, wsb, sp)
+            e1.record(stream)
+            if rc != 0:
+                raise RuntimeError(f'lddmm_apply_k failed: {rc}')
+            torch.cuda.synchronize()
+            if it >= warmup:
+                ms.append(e0.elapsed_time(e1))
+    t = statistics.mean(ms) * 1e-3
+    pps = n * n / t
+    return {'kernel': 'pairs_kernel_x<OpK, 128, 8> + finalize_kernel', 'ms_per_sum': t * 1e3, 'pairs_per_s': pps,
+            'sfu_frac': pps / 1e12 / peak_sfu, 'fp32_frac': 6 * pps / 1e12 / peak_fp32, 'sums_timed': len(ms),
+            'note': 'K(y,x)a with y a distinct copy of x: every ordered pair evaluated; the self-sum path above '
+                    'is faster per sum'}
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -997,6 +1028,9 @@ def run_b200(args, rank, world, local_rank):
         'clocks': clocks, 'gpu_launches': launches,
         'pairs_per_step': pairs_per_step,
     }
+    if world == 1:
+        line['ordered_pair_kernel'] = ordered_pair_kernel(X, A, lib, nat, ws, wsb, o, sp, flush, peak_fp32, peak_sfu,
+                                                          args.warmup)
     if world == 1 and not args.no_errors:
         line['errors'] = run_errors()
     if world == 1 and not args.no_registration:

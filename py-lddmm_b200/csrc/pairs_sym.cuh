@@ -46,6 +46,9 @@
 #ifndef LDDMM_SYMX_COL_SPLIT
 #define LDDMM_SYMX_COL_SPLIT 0  // 1: pairs_kernel_symx accumulates the column terms of even and odd lane groups apart
 #endif
+#ifndef LDDMM_SYMX_UNROLL
+#define LDDMM_SYMX_UNROLL 8  // unroll depth of pairs_kernel_symx's source loop (8: 1% faster than 4 at level 6)
+#endif
 #ifndef LDDMM_SYM_UNROLL
 #define LDDMM_SYM_UNROLL 4  // unroll depth of the 32-step source loop of a chunk (4: 1% faster than 2 at level 6)
 #endif
@@ -53,6 +56,7 @@
 namespace lddmm {
 
 constexpr int kSymUnroll = LDDMM_SYM_UNROLL;
+constexpr int kSymxUnroll = LDDMM_SYMX_UNROLL;
 
 // Shared-memory record of a staged source tile. In the symmetric kernels the 32 lanes of a warp read 32 different
 // sources at every step (no broadcast), so the record size is what the loads cost: compact records hold each field
@@ -405,7 +409,7 @@ __device__ __forceinline__ void symx_tile(const F2 (&yt)[RT / 2][3], const F2 (&
     float cs[NP];
 #pragma unroll
     for (int c = 0; c < NP; ++c) cs[c] = 0.f;
-#pragma unroll kSymUnroll
+#pragma unroll kSymxUnroll
     for (int s = 0; s < 32; ++s) {
       const int src = chunk * 32 + ((lane + s) & 31);
       F2 sv[St::kFields];
