@@ -224,8 +224,10 @@ int lddmm_bf16_gemm(int trans_a, int trans_b, int epilogue, int64_t M, int64_t N
                     const void* B, const float* bias, const void* mask, void* C, int splits, float* split_ws,
                     size_t split_ws_bytes, lddmm_stream_t stream);
 
-/* db(N) = column sums of dy (M,N) bf16, FP32, fixed order. */
-int lddmm_bf16_colsum(const void* dy, int64_t M, int64_t N, float* db, lddmm_stream_t stream);
+/* db(N) = column sums of dy (M,N) bf16, FP32, fixed order. With a workspace ws of at least ceil(M/256)*N floats
+ * the rows are split over the whole GPU (two stages, still fixed order); ws = NULL sums with N/32 CTAs. */
+int lddmm_bf16_colsum(const void* dy, int64_t M, int64_t N, float* db, float* ws, size_t ws_bytes,
+                      lddmm_stream_t stream);
 
 /* Squared-error gradient of the first nout columns of y (M,N) f32 against target (M,nout) f32 for rows < valid:
  * dy (M,N) bf16 = 2 w (y - target) there and 0 elsewhere; row_loss (M) f32 = per-row squared errors. */

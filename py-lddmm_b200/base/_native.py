@@ -59,7 +59,7 @@ SIGNATURES = {
                                _dp, _int, _vp, _sz, _vp],
     'lddmm_vertex_face_table': [_vp, _i64, _i64, _vp, _vp],
     'lddmm_bf16_gemm': [_int, _int, _int, _i64, _i64, _i64, _dp, _dp, _dp, _dp, _dp, _int, _dp, _sz, _vp],
-    'lddmm_bf16_colsum': [_dp, _i64, _i64, _dp, _vp],
+    'lddmm_bf16_colsum': [_dp, _i64, _i64, _dp, _dp, _sz, _vp],
     'lddmm_mse_grad': [_dp, _i64, _i64, _dp, _i64, _i64, ctypes.c_float, _dp, _dp, _vp],
     'lddmm_adam_step': [_dp, _dp, _dp, _dp, _dp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                         ctypes.c_float, _i64, ctypes.c_float, _vp],

@@ -54,6 +54,8 @@ MOMENTUM_LAW_SHAPES = ('a = (w1 q + w2 b + w3 K_0.4 z) n: q = x^T M x (M symmetr
                        'white noise, weights U[0,1], each field scaled to max 1; rescaled to a maximum initial speed '
                        'U[0.05, 0.35]; shot with sigma 0.5, T = 10')
 SCALAR_WIDTHS = (0.1, 0.2, 0.35, 0.7)
+# rows per split of the weight-gradient GEMMs (act^T dy, K = the batch's rows): split-K keeps the whole GPU busy
+SPLIT_ROWS = 512
 ROW_PAD = 64
 
 
@@ -172,8 +174,9 @@ class MomentumProposal:
         row_loss = torch.empty(M, dtype=torch.float32, device=F.device)
         nat.check(nat.lib().lddmm_mse_grad(nat.ptr(y), M, OUT_DIM, nat.ptr(target), N_OUT, int(valid), float(w),
                                            nat.ptr(dy), nat.ptr(row_loss), nat.stream_ptr()), 'mse_grad')
-        splits = max(1, min(64, M // 2048))
+        splits = max(1, min(64, M // SPLIT_ROWS))
         split_ws = torch.empty(splits * HIDDEN * HIDDEN, dtype=torch.float32, device=F.device) if splits > 1 else None
+        col_ws = torch.empty(((M + 255) // 256) * max(self.dims), dtype=torch.float32, device=F.device)
         dW, db = [None] * 4, [None] * 4
         for i in range(3, -1, -1):
             fi, fo = self.dims[i], self.dims[i + 1]
@@ -181,7 +184,8 @@ class MomentumProposal:
             sp = splits if split_ws is not None and fi * fo <= HIDDEN * HIDDEN else 1
             self._gemm(1, 0, 0, acts[i], dy, gw, fi, fo, M, splits=sp, split_ws=split_ws if sp > 1 else None)
             gb = torch.empty(fo, dtype=torch.float32, device=F.device)
-            nat.check(nat.lib().lddmm_bf16_colsum(nat.ptr(dy), M, fo, nat.ptr(gb), nat.stream_ptr()), 'colsum')
+            nat.check(nat.lib().lddmm_bf16_colsum(nat.ptr(dy), M, fo, nat.ptr(gb), nat.ptr(col_ws), col_ws.numel() * 4,
+                                                  nat.stream_ptr()), 'colsum')
             dW[i], db[i] = gw, gb
             if i > 0:
                 dx = torch.empty((M, fi), dtype=torch.bfloat16, device=F.device)

@@ -183,6 +183,36 @@ __global__ void colsum_kernel(const bf16* __restrict__ dy, int M, int N, float* 
   }
 }
 
+// Two-stage column sums for tall matrices: stage 1, one CTA per (32 columns, kColsumRows rows) writes the chunk's
+// column sums (8 row lanes x 32 columns, then the 8 lanes in order) to partial[chunk][col]; stage 2 adds the chunks
+// of each column in chunk order. Deterministic; the whole GPU takes part instead of N / 32 CTAs.
+constexpr int kColsumRows = 256;
+__global__ void colsum_partial_kernel(const bf16* __restrict__ dy, int M, int N, float* __restrict__ partial) {
+  __shared__ float red[8][33];
+  const int col = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int ry = threadIdx.x >> 5;
+  const int r0 = blockIdx.y * kColsumRows;
+  const int r1 = min(M, r0 + kColsumRows);
+  float s = 0.f;
+  if (col < N)
+    for (int m = r0 + ry; m < r1; m += 8) s += __bfloat162float(dy[(size_t)m * N + col]);
+  red[ry][threadIdx.x & 31] = s;
+  __syncthreads();
+  if (ry == 0 && col < N) {
+    float t = 0.f;
+    for (int k = 0; k < 8; ++k) t += red[k][threadIdx.x & 31];
+    partial[(size_t)blockIdx.y * N + col] = t;
+  }
+}
+
+__global__ void colsum_final_kernel(const float* __restrict__ partial, int chunks, int N, float* __restrict__ db) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= N) return;
+  float t = 0.f;
+  for (int c = 0; c < chunks; ++c) t += partial[(size_t)c * N + col];
+  db[col] = t;
+}
+
 // Squared-error gradient of the first `nout` output columns: dy = 2 w (y - target) for rows < valid, 0 elsewhere;
 // per-row losses go to `row_loss` (FP32) for a fixed-order reduction by the host.
 __global__ void mse_grad_kernel(const float* __restrict__ y, int M, int N, const float* __restrict__ target, int nout,
@@ -310,10 +340,20 @@ int lddmm_bf16_gemm(int trans_a, int trans_b, int epilogue, int64_t M, int64_t N
   return kOk;
 }
 
-int lddmm_bf16_colsum(const void* dy, int64_t M, int64_t N, float* db, lddmm_stream_t stream) {
+int lddmm_bf16_colsum(const void* dy, int64_t M, int64_t N, float* db, float* ws, size_t ws_bytes,
+                      lddmm_stream_t stream) {
   if (M < 0 || N <= 0 || dy == nullptr || db == nullptr || M > INT32_MAX || N > INT32_MAX) return kInvalidArgument;
-  colsum_kernel<<<(unsigned)((N + 31) / 32), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const bf16*>(dy),
-                                                                             (int)M, (int)N, db);
+  const int64_t chunks = (M + kColsumRows - 1) / kColsumRows;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ws == nullptr || chunks <= 1) {
+    colsum_kernel<<<(unsigned)((N + 31) / 32), 256, 0, st>>>(reinterpret_cast<const bf16*>(dy), (int)M, (int)N, db);
+  } else {
+    if (ws_bytes < (size_t)chunks * (size_t)N * sizeof(float)) return kWorkspaceTooSmall;
+    if (chunks > 65535) return kInvalidArgument;
+    colsum_partial_kernel<<<dim3((unsigned)((N + 31) / 32), (unsigned)chunks), 256, 0, st>>>(
+        reinterpret_cast<const bf16*>(dy), (int)M, (int)N, ws);
+    colsum_final_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(ws, (int)chunks, (int)N, db);
+  }
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
