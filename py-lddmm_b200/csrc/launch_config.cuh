@@ -23,6 +23,15 @@
 #ifndef LDDMM_RT_FO_SYM
 #define LDDMM_RT_FO_SYM 4
 #endif
+#ifndef LDDMM_RT_SYM_FWD_L
+#define LDDMM_RT_SYM_FWD_L 4
+#endif
+#ifndef LDDMM_RT_ADJOINT_SYM_L
+#define LDDMM_RT_ADJOINT_SYM_L 2
+#endif
+#ifndef LDDMM_RT_FO_SYM_L
+#define LDDMM_RT_FO_SYM_L 4
+#endif
 #ifndef LDDMM_TPB_KSYM
 #define LDDMM_TPB_KSYM 128
 #endif
@@ -56,6 +65,11 @@ constexpr int kRtSymFwd = LDDMM_RT_SYM_FWD;
 // The symmetric K(x, x) a (pairs_kernel_symx): 8 targets per thread.
 // The symmetric first-order adjoint step (pairs_kernel_sym): 4 targets per thread.
 constexpr int kRtFoSym = LDDMM_RT_FO_SYM;
+// The symmetric steps with the Laplacian family (its radial profile -- a square root and the polynomial -- takes
+// registers that the Gaussian shapes spend on more targets per thread).
+constexpr int kRtSymFwdL = LDDMM_RT_SYM_FWD_L;
+constexpr int kRtAdjointSymL = LDDMM_RT_ADJOINT_SYM_L;
+constexpr int kRtFoSymL = LDDMM_RT_FO_SYM_L;
 constexpr int kTpbKSym = LDDMM_TPB_KSYM;
 constexpr int kRtKSym = LDDMM_RT_KSYM;
 // FP64 baseline path.

@@ -149,7 +149,7 @@ inline SymPlan make_sym_plan(int64_t n, int nr, int nc, int ctas_per_sm) {
   return p;
 }
 
-template <class Op, int TPB, int RT, bool COL>
+template <class Op, int TPB, int RT, bool COL, class Fam>
 __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymTgt (&tgt)[RT / 2],
                                          const typename SymStage<Op::NSS, TPB>::T (*sm)[TPB], float (*colacc)[TPB],
                                          F2 (&acc)[RT / 2][Op::NR]) {
@@ -172,7 +172,7 @@ __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymT
 #pragma unroll
         for (int c = 0; c < Op::NC; ++c) col[c] = f2(cs[c], 0.f);
 #pragma unroll
-        for (int g = 0; g < G; ++g) Op::template pair_sym<true>(f, tgt[g], sv, acc[g], col);
+        for (int g = 0; g < G; ++g) Op::template pair_sym<true, Fam>(f, tgt[g], sv, acc[g], col);
 #pragma unroll
         for (int c = 0; c < Op::NC; ++c) {
           float lo, hi;
@@ -181,7 +181,7 @@ __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymT
         }
       } else {
 #pragma unroll
-        for (int g = 0; g < G; ++g) Op::template pair_sym<false>(f, tgt[g], sv, acc[g], nullptr);
+        for (int g = 0; g < G; ++g) Op::template pair_sym<false, Fam>(f, tgt[g], sv, acc[g], nullptr);
       }
     }
     if constexpr (COL) {
@@ -192,7 +192,7 @@ __device__ __forceinline__ void sym_tile(const Frame& f, const typename Op::SymT
   }
 }
 
-template <class Op, int TPB, int RT>
+template <class Op, int TPB, int RT, class Fam = Gauss>
 __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
     pairs_kernel_sym(const typename Op::Params P, int n, int nblk, int TT, long long U, int C,
                      float2* __restrict__ row_ws, float* __restrict__ col_ws) {
@@ -250,9 +250,9 @@ __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
 #pragma unroll
         for (int c = 0; c < NR; ++c) acc[g][c] = VT<F2>::zero();
       if (diag)
-        sym_tile<Op, TPB, RT, false>(f, tgt, sm, colacc, acc);
+        sym_tile<Op, TPB, RT, false, Fam>(f, tgt, sm, colacc, acc);
       else
-        sym_tile<Op, TPB, RT, true>(f, tgt, sm, colacc, acc);
+        sym_tile<Op, TPB, RT, true, Fam>(f, tgt, sm, colacc, acc);
 #pragma unroll
       for (int g = 0; g < G; ++g)
 #pragma unroll
@@ -324,7 +324,7 @@ constexpr size_t sym_dyn_smem_bytes() {
 
 // Declare the kernel's dynamic shared memory, once per device (the attribute belongs to the device's context):
 // without it static + dynamic shared memory may not exceed 48 KiB. Returns false when the device refuses.
-template <class Op, int TPB, int RT>
+template <class Op, int TPB, int RT, class Fam = Gauss>
 inline bool sym_prepare() {
   static signed char state[64] = {};
   int dev = 0;
@@ -334,7 +334,7 @@ inline bool sym_prepare() {
   }
   if (dev < 0 || dev >= 64) return false;
   if (state[dev] == 0) {
-    const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT>),
+    const cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT, Fam>),
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)sym_dyn_smem_bytes<Op, TPB, RT>());
     if (e != cudaSuccess) cudaGetLastError();
@@ -343,34 +343,34 @@ inline bool sym_prepare() {
   return state[dev] > 0;
 }
 
-template <class Op, int TPB, int RT>
+template <class Op, int TPB, int RT, class Fam = Gauss>
 inline int sym_ctas_per_sm() {
   static int cached = 0;
   if (cached == 0) {
-    sym_prepare<Op, TPB, RT>();
-    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT>), TPB,
+    sym_prepare<Op, TPB, RT, Fam>();
+    int c = resident_ctas(reinterpret_cast<const void*>(&pairs_kernel_sym<Op, TPB, RT, Fam>), TPB,
                           sym_dyn_smem_bytes<Op, TPB, RT>());
     cached = c > 0 ? c : 2;
   }
   return cached;
 }
 
-template <class Op, int TPB, int RT>
+template <class Op, int TPB, int RT, class Fam = Gauss>
 inline size_t sym_ws_bytes(int64_t n) {
-  return make_sym_plan<TPB, RT>(n, Op::NR, Op::NC, sym_ctas_per_sm<Op, TPB, RT>()).ws_bytes;
+  return make_sym_plan<TPB, RT>(n, Op::NR, Op::NC, sym_ctas_per_sm<Op, TPB, RT, Fam>()).ws_bytes;
 }
 
-template <class Op, int TPB, int RT>
+template <class Op, int TPB, int RT, class Fam = Gauss>
 inline int run_pairs_sym(const typename Op::Params& P, int64_t n, void* ws, size_t ws_bytes, cudaStream_t stream) {
   if (n <= 0) return kOk;
   if (n > INT32_MAX / 4) return kInvalidArgument;
-  const SymPlan plan = make_sym_plan<TPB, RT>(n, Op::NR, Op::NC, sym_ctas_per_sm<Op, TPB, RT>());
+  const SymPlan plan = make_sym_plan<TPB, RT>(n, Op::NR, Op::NC, sym_ctas_per_sm<Op, TPB, RT, Fam>());
   if (plan.ws_bytes > ws_bytes) return kWorkspaceTooSmall;
   if (ws == nullptr) return kInvalidArgument;
-  if (!sym_prepare<Op, TPB, RT>()) return kLaunchFailure;
+  if (!sym_prepare<Op, TPB, RT, Fam>()) return kLaunchFailure;
   auto* row_ws = reinterpret_cast<float2*>(ws);
   auto* col_ws = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.col_off);
-  pairs_kernel_sym<Op, TPB, RT><<<plan.C, TPB, sym_dyn_smem_bytes<Op, TPB, RT>(), stream>>>(
+  pairs_kernel_sym<Op, TPB, RT, Fam><<<plan.C, TPB, sym_dyn_smem_bytes<Op, TPB, RT>(), stream>>>(
       P, (int)n, plan.nblk, plan.TT, plan.U, plan.C, row_ws, col_ws);
   const int fb = 256;
   finalize_sym_kernel<Op, TPB, RT><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT, plan.U,

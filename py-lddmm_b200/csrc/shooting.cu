@@ -228,21 +228,22 @@ struct OpSOFwdSym {
   static __device__ __forceinline__ void source_fields_sym(const Params& P, int l, double* f) {
     OpSOFwd::source_fields(P, l, f);
   }
-  template <bool COL>
-  static __device__ __forceinline__ void pair_sym(const Frame&, const SymTgt& t, const F2* s, F2* row, F2* col) {
+  // Fam: the radial factors k0 (K a) and k1 (the momentum term); both are e for the Gaussian
+  template <bool COL, class Fam>
+  static __device__ __forceinline__ void pair_sym(const Frame& f, const SymTgt& t, const F2* s, F2* row, F2* col) {
     const F2 d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const F2 e = VT<F2>::expneg(sqdist(d0, d1, d2));
-    const F2 ec = e * dot3(t.a0, t.a1, t.a2, s[3], s[4], s[5]);
-    row[0] = fma(e, s[3], row[0]);
-    row[1] = fma(e, s[4], row[1]);
-    row[2] = fma(e, s[5], row[2]);
+    const KV<F2> k = Fam::template eval<F2>(f, sqdist(d0, d1, d2));
+    const F2 ec = k.k1 * dot3(t.a0, t.a1, t.a2, s[3], s[4], s[5]);
+    row[0] = fma(k.k0, s[3], row[0]);
+    row[1] = fma(k.k0, s[4], row[1]);
+    row[2] = fma(k.k0, s[5], row[2]);
     row[3] = fma(ec, d0, row[3]);
     row[4] = fma(ec, d1, row[4]);
     row[5] = fma(ec, d2, row[5]);
     if constexpr (COL) {
-      col[0] = fma(e, t.a0, col[0]);
-      col[1] = fma(e, t.a1, col[1]);
-      col[2] = fma(e, t.a2, col[2]);
+      col[0] = fma(k.k0, t.a0, col[0]);
+      col[1] = fma(k.k0, t.a1, col[1]);
+      col[2] = fma(k.k0, t.a2, col[2]);
       col[3] = fma(ec, d0, col[3]);
       col[4] = fma(ec, d1, col[4]);
       col[5] = fma(ec, d2, col[5]);
@@ -291,32 +292,35 @@ struct OpSOBwdSym {
   static __device__ __forceinline__ void source_fields_sym(const Params& P, int l, double* f) {
     OpSOBwd::source_fields(P, l, f);
   }
-  template <bool COL>
-  static __device__ __forceinline__ void pair_sym(const Frame&, const SymTgt& t, const F2* s, F2* row, F2* col) {
+  // Fam: the radial factors k0 (the px'-sum), k1 (first-derivative terms) and k2 (the second-derivative term
+  // c2 dq d); all three are e for the Gaussian, where k1 c2 and k2 c2 are one product
+  template <bool COL, class Fam>
+  static __device__ __forceinline__ void pair_sym(const Frame& f, const SymTgt& t, const F2* s, F2* row, F2* col) {
     const F2 d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const F2 e = VT<F2>::expneg(sqdist(d0, d1, d2));
+    const KV<F2> k = Fam::template eval<F2>(f, sqdist(d0, d1, d2));
     const F2 w0 = t.q0 - s[6], w1 = t.q1 - s[7], w2 = t.q2 - s[8];
     const F2 dq = dot3(d0, d1, d2, w0, w1, w2);
     const F2 c1 = fma(t.a2, s[11], fma(t.a1, s[10], fma(t.a0, s[9], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
-    const F2 ec2 = e * dot3(t.b0, t.b1, t.b2, s[3], s[4], s[5]);
-    const F2 eg = fma(ec2, dq, e * c1);
+    const F2 c2 = dot3(t.b0, t.b1, t.b2, s[3], s[4], s[5]);
+    const F2 ec2 = k.k1 * c2;
+    const F2 eg = fma(k.k2 * c2, dq, k.k1 * c1);
     const F2 tw = ec2 * t.cd;
     const F2 v0 = fma(tw, w0, eg * d0), v1 = fma(tw, w1, eg * d1), v2 = fma(tw, w2, eg * d2);
     row[0] += v0;
     row[1] += v1;
     row[2] += v2;
-    const F2 edq = e * dq;
+    const F2 edq = k.k1 * dq;
     const F2 edqk = edq * t.k2;
-    row[3] = fma(edqk, s[3], fma(e, s[9], row[3]));
-    row[4] = fma(edqk, s[4], fma(e, s[10], row[4]));
-    row[5] = fma(edqk, s[5], fma(e, s[11], row[5]));
+    row[3] = fma(edqk, s[3], fma(k.k0, s[9], row[3]));
+    row[4] = fma(edqk, s[4], fma(k.k0, s[10], row[4]));
+    row[5] = fma(edqk, s[5], fma(k.k0, s[11], row[5]));
     if constexpr (COL) {
       col[0] += v0;
       col[1] += v1;
       col[2] += v2;
-      col[3] = fma(edq, t.b0, fma(e, t.p0, col[3]));
-      col[4] = fma(edq, t.b1, fma(e, t.p1, col[4]));
-      col[5] = fma(edq, t.b2, fma(e, t.p2, col[5]));
+      col[3] = fma(edq, t.b0, fma(k.k0, t.p0, col[3]));
+      col[4] = fma(edq, t.b1, fma(k.k0, t.p1, col[4]));
+      col[5] = fma(edq, t.b2, fma(k.k0, t.p2, col[5]));
     }
   }
   // zpx = row - col (the mirrored px-sum changes sign), zpa = -(row + col) / kappa
@@ -419,25 +423,26 @@ struct OpFOBwdSym {
   static __device__ __forceinline__ void source_fields_sym(const Params& P, int l, double* f) {
     OpFOBwd::source_fields(P, l, f);
   }
-  template <bool COL>
-  static __device__ __forceinline__ void pair_sym(const Frame&, const SymTgt& t, const F2* s, F2* row, F2* col) {
+  // Fam: k1 for the adjoint term, k0 for the Q sum (both e for the Gaussian)
+  template <bool COL, class Fam>
+  static __device__ __forceinline__ void pair_sym(const Frame& f, const SymTgt& t, const F2* s, F2* row, F2* col) {
     const F2 d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
-    const F2 e = VT<F2>::expneg(sqdist(d0, d1, d2));
+    const KV<F2> k = Fam::template eval<F2>(f, sqdist(d0, d1, d2));
     const F2 c = fma(t.a2, s[8], fma(t.a1, s[7], fma(t.a0, s[6], dot3(t.p0, t.p1, t.p2, s[3], s[4], s[5]))));
-    const F2 ec = e * c;
+    const F2 ec = k.k1 * c;
     row[0] = fma(ec, d0, row[0]);
     row[1] = fma(ec, d1, row[1]);
     row[2] = fma(ec, d2, row[2]);
-    row[3] = fma(e, s[6], row[3]);
-    row[4] = fma(e, s[7], row[4]);
-    row[5] = fma(e, s[8], row[5]);
+    row[3] = fma(k.k0, s[6], row[3]);
+    row[4] = fma(k.k0, s[7], row[4]);
+    row[5] = fma(k.k0, s[8], row[5]);
     if constexpr (COL) {
       col[0] = fma(ec, d0, col[0]);
       col[1] = fma(ec, d1, col[1]);
       col[2] = fma(ec, d2, col[2]);
-      col[3] = fma(e, t.q0, col[3]);
-      col[4] = fma(e, t.q1, col[4]);
-      col[5] = fma(e, t.q2, col[5]);
+      col[3] = fma(k.k0, t.q0, col[3]);
+      col[4] = fma(k.k0, t.q1, col[4]);
+      col[5] = fma(k.k0, t.q2, col[5]);
     }
   }
   // A = row - col (the mirrored difference changes sign), Q = row + col
@@ -456,6 +461,9 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
       upd(sym_ws_bytes<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(n));
       upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymFwd>(n));
       upd(sym_ws_bytes<OpFOBwdSym, kTpbLight, kRtFoSym>(n));
+      upd(sym_ws_bytes<OpSOBwdSym, kTpbHeavy, kRtAdjointSymL, Laplacian>(n));
+      upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymFwdL, Laplacian>(n));
+      upd(sym_ws_bytes<OpFOBwdSym, kTpbLight, kRtFoSymL, Laplacian>(n));
       upd(symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n));
     }
     upd(pairs_ws_bytes_any<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
@@ -535,7 +543,10 @@ int so_step(const double* x, const double* a, int64_t n, const Frame& f, double 
   OpSOFwd::Params P{x, a, x1, a1, f, dt, (int)row0};
   const int64_t rows = nrows < 0 ? n : nrows;
   if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
-    if (f.family == kGauss && row0 == 0 && rows == n) return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymFwd>(P, n, ws, wsb, st);
+    if (row0 == 0 && rows == n) {
+      if (f.family == kGauss) return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymFwd>(P, n, ws, wsb, st);
+      return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymFwdL, Laplacian>(P, n, ws, wsb, st);
+    }
   }
   return run_pairs_k<OpSOFwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, rows, n, ws, wsb, st);
 }
@@ -547,7 +558,10 @@ int so_adjoint_step(const double* x, const double* a, const double* px, const do
   OpSOBwd::Params P{x, a, px, pa, px_prev, pa_prev, f, dt, (int)row0};
   const int64_t rows = nrows < 0 ? n : nrows;
   if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
-    if (f.family == kGauss && row0 == 0 && rows == n) return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(P, n, ws, wsb, st);
+    if (row0 == 0 && rows == n) {
+      if (f.family == kGauss) return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(P, n, ws, wsb, st);
+      return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtAdjointSymL, Laplacian>(P, n, ws, wsb, st);
+    }
   }
   if (f.family == kGauss) return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtH, Gauss>(P, rows, n, ws, wsb, st);
   return run_pairs<OpSOBwd, V, Shape<V>::kTpbH, Shape<V>::kRtHL, Laplacian>(P, rows, n, ws, wsb, st);
@@ -617,7 +631,7 @@ int fo_gradient(const double* xt, const double* at, int64_t n, int64_t T, const 
     int rc;
     if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
       rc = f.family == kGauss ? run_pairs_sym<OpFOBwdSym, kTpbLight, kRtFoSym>(P, n, ws, wsb, st)
-                              : run_pairs_k<OpFOBwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
+                              : run_pairs_sym<OpFOBwdSym, kTpbLight, kRtFoSymL, Laplacian>(P, n, ws, wsb, st);
     } else {
       rc = run_pairs_k<OpFOBwd, V, Shape<V>::kTpb, Shape<V>::kRt>(P, n, n, ws, wsb, st);
     }

@@ -96,6 +96,30 @@ def test_laplacian_l4_vs_oracle(order):
     assert all(e < 2e-5 for e in errs.values()), errs
 
 
+@pytest.mark.parametrize('order', [1, 3])
+def test_laplacian_first_order_l4_vs_oracle(order):
+    """First-order shooting and adjoint with the Laplacian kernel at level 4 (several row blocks of the symmetric
+    adjoint step), FP32 against the oracle: trajectory, covectors and the gradient (relative L2 2e-5)."""
+    import torch
+    import oracle as O
+    from base import pointEvolution as evol
+    from base.syntheticShapes import icosphere
+    L = O.laplacian
+    x0, _ = icosphere(4)
+    rng = np.random.default_rng(31 + order)
+    T, w = 4, 0.7
+    at = np.stack([O.apply_k(x0, x0, rng.normal(0, 0.02, x0.shape), 0.3) for _ in range(T)])
+    px1 = rng.normal(size=x0.shape)
+    K = kernel(0.4, order, 'float32')
+    AT = torch.from_numpy(at).cuda()
+    xt = evol.shoot_first_order(torch.from_numpy(x0).cuda(), AT, K, regweight=w)
+    dat_ref, xt_ref, pxt_ref = O.landmark_hamiltonian_gradient(x0, at, px1, 0.4, w, L.ops(order))
+    assert rel_err(xt.cpu().numpy() - x0, xt_ref - x0) < 2e-5
+    pxt, dat = evol.first_order_gradient(xt, AT, torch.from_numpy(px1).cuda(), K, w)
+    assert rel_err(pxt.cpu().numpy() - px1, pxt_ref - px1) < 2e-5
+    assert rel_err(dat.cpu().numpy(), dat_ref) < 2e-5
+
+
 def test_laplacian_multiscale_and_dense_matrix():
     """Two widths weighted sigma^-1 / sum sigma^-1 (base/kernelFunctions_util.py:451-466) and getK."""
     import oracle as O
