@@ -104,6 +104,45 @@ struct OpKSym {
   }
 };
 
+// K(x, x) a evaluated once per unordered pair in the difference form (pairs_kernel_sym), for kernel families
+// without an expanded form (the Laplacian): row term k0 a_l, column term k0 a_k. The epilogue options of OpK apply.
+struct OpKSymD {
+  using Params = OpK::Params;
+  static constexpr int NSS = 6, NR = 3, NC = 3;
+  static constexpr int kSymMinCtas = LDDMM_KSYM_MIN_CTAS;
+  struct SymTgt { F2 y0, y1, y2, a0, a1, a2; };
+  static __device__ __forceinline__ void load_target_sym(const Params& P, int i0, int i1, bool v0, bool v1,
+                                                         SymTgt& t) {
+    t.y0 = tgt_coord<F2>(P.x, i0, i1, 0, P.f.o0, P.f.s);
+    t.y1 = tgt_coord<F2>(P.x, i0, i1, 1, P.f.o1, P.f.s);
+    t.y2 = tgt_coord<F2>(P.x, i0, i1, 2, P.f.o2, P.f.s);
+    t.a0 = VT<F2>::pack(v0 ? P.a[3 * i0] : 0.0, v1 ? P.a[3 * i1] : 0.0);
+    t.a1 = VT<F2>::pack(v0 ? P.a[3 * i0 + 1] : 0.0, v1 ? P.a[3 * i1 + 1] : 0.0);
+    t.a2 = VT<F2>::pack(v0 ? P.a[3 * i0 + 2] : 0.0, v1 ? P.a[3 * i1 + 2] : 0.0);
+  }
+  // fields: x' (0-2), a (3-5)
+  static __device__ __forceinline__ void source_fields_sym(const Params& P, int l, double* f) {
+    OpK::source_fields(P, l, f);
+  }
+  template <bool COL, class Fam>
+  static __device__ __forceinline__ void pair_sym(const Frame& f, const SymTgt& t, const F2* s, F2* row, F2* col) {
+    const F2 d0 = t.y0 - s[0], d1 = t.y1 - s[1], d2 = t.y2 - s[2];
+    const KV<F2> k = Fam::template eval<F2>(f, sqdist(d0, d1, d2));
+    row[0] = fma(k.k0, s[3], row[0]);
+    row[1] = fma(k.k0, s[4], row[1]);
+    row[2] = fma(k.k0, s[5], row[2]);
+    if constexpr (COL) {
+      col[0] = fma(k.k0, t.a0, col[0]);
+      col[1] = fma(k.k0, t.a1, col[1]);
+      col[2] = fma(k.k0, t.a2, col[2]);
+    }
+  }
+  static __device__ __forceinline__ void finalize_sym(const Params& P, int i, const double* row, const double* col) {
+    const double acc[3] = {row[0] + col[0], row[1] + col[1], row[2] + col[2]};
+    OpK::finalize(P, i, acc);
+  }
+};
+
 // DK^T(y, x; p, a) -- base/kernelFunctions_util.py:773-793 with gauss_fun_diffT (:233).
 //   MODE 0 (plain): c = p_k.a_l                         13 FP32 + 1 SFU
 //   MODE 1 (sym)  : c = p_k.a_l + a_k.p_l               16 FP32 + 1 SFU

@@ -83,7 +83,10 @@ size_t kernel_sums_ws_bytes(int64_t n, int64_t m, int precision) {
   upd(op_ws<OpDiffK1and2, kTpbLight, kRtLight>(n, m, precision));
   upd(op_ws<OpDiv, kTpbLight, kRtLight>(n, m, precision));
   upd(op_ws<OpKTensor, kTpbLight, kRtLight>(n, m, precision));
-  if (LDDMM_SYM && precision == kFP32Compensated && n == m) upd(symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n));
+  if (LDDMM_SYM && precision == kFP32Compensated && n == m) {
+    upd(symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n));
+    upd(sym_ws_bytes<OpKSymD, kTpbLight, kRtKSymL, Laplacian>(n));
+  }
   return b;
 }
 
@@ -98,11 +101,12 @@ int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, 
   if (n < 0 || m < 0 || bad_sigma(sigma) || bad_ptr(y, n) || bad_ptr(out, n) || bad_ptr(x, m) || bad_ptr(a, m))
     return kInvalidArgument;
   // a self-sum K(x, x) a (the same point array as targets and sources): each unordered pair once
-  if (LDDMM_SYM && precision == kFP32Compensated && kernel == kGauss && y == x && n == m) {
+  if (LDDMM_SYM && precision == kFP32Compensated && y == x && n == m && !bad_kernel(kernel)) {
     OpK::Params P;
     P.f = make_frame(origin, sigma, kernel, true);
     P.y = y; P.x = x; P.a = a; P.out = out;
-    return run_pairs_symx<OpKSym, kTpbKSym, kRtKSym>(P, n, ws, wsb, (cudaStream_t)stream);
+    if (kernel == kGauss) return run_pairs_symx<OpKSym, kTpbKSym, kRtKSym>(P, n, ws, wsb, (cudaStream_t)stream);
+    return run_pairs_sym<OpKSymD, kTpbLight, kRtKSymL, Laplacian>(P, n, ws, wsb, (cudaStream_t)stream);
   }
   return dispatch<OpK, kTpbLight, kRtLight>(precision, n, m, sigma, kernel, origin, ws, wsb, (cudaStream_t)stream,
                                             [&](OpK::Params& P) { P.y = y; P.x = x; P.a = a; P.out = out; });

@@ -32,6 +32,9 @@
 #ifndef LDDMM_RT_FO_SYM_L
 #define LDDMM_RT_FO_SYM_L 4
 #endif
+#ifndef LDDMM_RT_KSYM_L
+#define LDDMM_RT_KSYM_L 4
+#endif
 #ifndef LDDMM_TPB_KSYM
 #define LDDMM_TPB_KSYM 128
 #endif
@@ -70,6 +73,7 @@ constexpr int kRtFoSym = LDDMM_RT_FO_SYM;
 constexpr int kRtSymFwdL = LDDMM_RT_SYM_FWD_L;
 constexpr int kRtAdjointSymL = LDDMM_RT_ADJOINT_SYM_L;
 constexpr int kRtFoSymL = LDDMM_RT_FO_SYM_L;
+constexpr int kRtKSymL = LDDMM_RT_KSYM_L;
 constexpr int kTpbKSym = LDDMM_TPB_KSYM;
 constexpr int kRtKSym = LDDMM_RT_KSYM;
 // FP64 baseline path.

@@ -465,6 +465,7 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
       upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymFwdL, Laplacian>(n));
       upd(sym_ws_bytes<OpFOBwdSym, kTpbLight, kRtFoSymL, Laplacian>(n));
       upd(symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n));
+      upd(sym_ws_bytes<OpKSymD, kTpbLight, kRtKSymL, Laplacian>(n));
     }
     upd(pairs_ws_bytes_any<OpSOFwd, F2, kTpbLight, kRtLight>(n, n));
     upd(pairs_ws_bytes<OpSOBwd, F2, kTpbHeavy, kRtAdjoint, Gauss>(n, n));
@@ -513,10 +514,13 @@ int k_energy_and_update(const double* x, const double* a, int64_t n, const Frame
   OpK::Params P;
   P.y = x; P.x = x; P.a = a; P.out = out; P.f = f;
   P.base = base; P.base_sign = base_sign; P.scale = scale;
-  // K(x) a is a self-sum: FP32 Gaussian sums evaluate each unordered pair once (pairs_kernel_symx)
+  // K(x) a is a self-sum: FP32 sums evaluate each unordered pair once (pairs_kernel_symx for the Gaussian,
+  // pairs_kernel_sym in the difference form for the Laplacian)
   constexpr bool kSymOk = std::is_same<V, F2>::value && LDDMM_SYM != 0;
-  const bool sym = kSymOk && f.family == kGauss;
-  const size_t pb = sym ? symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n) : pairs_ws_bytes_any<OpK, V, TPB, RT>(n, n);
+  const bool gauss = f.family == kGauss;
+  const size_t pb = !kSymOk ? pairs_ws_bytes_any<OpK, V, TPB, RT>(n, n)
+                    : gauss ? symx_ws_bytes<OpKSym, kTpbKSym, kRtKSym>(n)
+                            : sym_ws_bytes<OpKSymD, kTpbLight, kRtKSymL, Laplacian>(n);
   if (energy) {
     if (((pb + 255) & ~(size_t)255) + (size_t)n * sizeof(double) > wsb) return kWorkspaceTooSmall;
     P.dotw = dotw;
@@ -524,8 +528,8 @@ int k_energy_and_update(const double* x, const double* a, int64_t n, const Frame
   }
   int rc;
   if constexpr (kSymOk) {
-    rc = sym ? run_pairs_symx<OpKSym, kTpbKSym, kRtKSym>(P, n, ws, wsb, st) : run_pairs_k<OpK, V, TPB, RT>(P, n, n, ws,
-                                                                                                         wsb, st);
+    rc = gauss ? run_pairs_symx<OpKSym, kTpbKSym, kRtKSym>(P, n, ws, wsb, st)
+               : run_pairs_sym<OpKSymD, kTpbLight, kRtKSymL, Laplacian>(P, n, ws, wsb, st);
   } else {
     rc = run_pairs_k<OpK, V, TPB, RT>(P, n, n, ws, wsb, st);
   }

@@ -120,23 +120,32 @@ def test_ragged_and_edge_sizes(n, m):
         assert rel_err(K.applyDiffKT(x, p, a, firstVar=y), O.apply_diff_kt(y, x, p, a, 0.7)) < 2e-5
 
 
-@pytest.mark.parametrize('n', [1, 7, 1023, 1024, 1025, 2049, 5000])
+@pytest.mark.parametrize('family', ['gauss', 'laplacian'])
+@pytest.mark.parametrize('n', [1, 7, 511, 513, 1023, 1024, 1025, 2049, 5000])
 @pytest.mark.parametrize('spread', ['ball', 'wide'])
-def test_self_sum_ragged_sizes(n, spread):
-    """K(x, x) a with one point array as targets and sources runs the symmetric kernel (each unordered pair once,
-    credited to both points; 1,024 points per block): sizes below, at and above one and two blocks, points in a
-    small ball (expanded-distance form) or spread far in kernel widths (difference form for wide blocks), against
-    the oracle and against the ordered-pair kernel (the same sum through a distinct target array)."""
+def test_self_sum_ragged_sizes(n, spread, family):
+    """K(x, x) a with one point array as targets and sources runs a symmetric kernel (each unordered pair once,
+    credited to both points; Gaussian: 1,024 points per block, Laplacian: 512): sizes below, at and above one and
+    two blocks, points in a small ball (Gaussian: expanded-distance form) or spread far in kernel widths (difference
+    form for wide blocks), against the oracle and against the ordered-pair kernel (the same sum through a distinct
+    target array)."""
     import oracle as O
+    from base.kernelFunctions import Kernel
     rng = np.random.default_rng(n)
     scale = 0.5 if spread == 'ball' else 6.0
     x = rng.normal(size=(n, 3)) * scale
     a = rng.normal(size=(n, 3))
-    K = kernel(0.7, 'float32')
+    if family == 'gauss':
+        K = kernel(0.7, 'float32')
+        ref = O.apply_k(x, x, a, 0.7)
+    else:   # Laplacian of order 3: the difference-form symmetric kernel (row blocks of 512 points)
+        K = Kernel(name='laplacian', sigma=0.7, order=3)
+        K.pk_dtype = 'float32'
+        ref = O.laplacian.apply_k(x, x, a, 0.7, 3)
     out = K.applyK(x, a)
-    ref = O.apply_k(x, x, a, 0.7)
-    assert rel_err(out, ref) < 2e-5
-    assert rel_err(K.applyK(x, a, firstVar=x.copy()), ref) < 2e-5
+    tol = 2e-5 if family == 'gauss' else 3e-5     # random-sign momenta: cancellation (Laplacian: its polynomial too)
+    assert rel_err(out, ref) < tol
+    assert rel_err(K.applyK(x, a, firstVar=x.copy()), ref) < tol
 
 
 def test_full_size_properties_l6():
