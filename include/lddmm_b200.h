@@ -64,7 +64,10 @@ size_t lddmm_workspace_bytes(int64_t n_max, int64_t m_max, int precision);
  * LDDMM_KERNEL_LAPLACIAN(order) (LDDMM_ERR_INVALID_ARGUMENT otherwise).
  * ------------------------------------------------------------------------------------------------------- */
 
-/* out(n,3) = K(y, x) a.  Kernel.applyK(x, a, firstVar=y)  base/kernelFunctions.py:452. */
+/* out(n,3) = K(y, x) a.  Kernel.applyK(x, a, firstVar=y)  base/kernelFunctions.py:452.
+ * When y == x (the same pointer) and n == m, FP32 evaluates the self-sum once per unordered pair (symmetric
+ * kernel; the workspace of lddmm_workspace_bytes(n, n, ...) covers it); results agree with the ordered-pair
+ * evaluation to FP32 rounding. */
 int lddmm_apply_k(const double* y, int64_t n, const double* x, const double* a, int64_t m, double sigma, int kernel,
                   const double* origin, double* out, int precision, void* workspace, size_t workspace_bytes,
                   lddmm_stream_t stream);

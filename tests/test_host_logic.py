@@ -134,3 +134,59 @@ def test_working_gradient_converges():
     bfgs_mod.bfgs(m, verb=False, maxIter=50, epsInit=1.0, Wolfe=True, lineSearch='Weak_Wolfe', memory=5)
     assert float((m.control['a0'] - m.c).abs().max()) < 1e-6
     assert m.options['KparDiff'].pk_dtype == 'float32'
+
+
+class _IllConditioned(QuadraticMatching):
+    """0.5 (a - c)^T D (a - c) with D spread over two decades: BFGS needs several iterations and keeps pairs."""
+
+    def __init__(self, hook=None):
+        super().__init__()
+        self.D = torch.logspace(-1, 1, 3 * self.npt, dtype=torch.float64).reshape(self.npt, 3)
+        self.hook = hook
+        self.hook_calls = 0
+
+    def objectiveFunDef(self, control, var=None, withTrajectory=True, withJacobian=False):
+        self.evaluations += 1
+        a = control['a0']
+        return 0.5 * float((self.D * (a - self.c) ** 2).sum()), State(xt=torch.zeros((2, self.npt, 3),
+                                                                                      dtype=torch.float64))
+
+    def _gradient(self, coeff=1.0, update=None):
+        a = self.control['a0'] if update is None else self.control['a0'] - update[1] * update[0]['a0']
+        return Control(a0=self.D * (a - self.c) / coeff)
+
+    def lbfgs_direction(self, grd, history):
+        self.hook_calls += 1
+        return None if self.hook is None else self.hook(grd, history)
+
+
+def _compact_lbfgs(grd, history):
+    """H g by the compact representation of L-BFGS (Byrd, Nocedal and Schnabel 1994) -- mathematically the two-loop
+    recursion with H0 = gamma I, gamma = s.y / y.y of the newest pair, computed another way."""
+    g = grd['a0'].reshape(-1).numpy()
+    S = np.stack([h[0]['a0'].reshape(-1).numpy() for h in history], axis=1)
+    Y = np.stack([h[1]['a0'].reshape(-1).numpy() for h in history], axis=1)
+    gamma = (S[:, -1] @ Y[:, -1]) / (Y[:, -1] @ Y[:, -1])
+    SY = S.T @ Y
+    R = np.triu(SY)
+    Dm = np.diag(np.diag(SY))
+    Rinv = np.linalg.inv(R)
+    M = np.block([[Rinv.T @ (Dm + gamma * Y.T @ Y) @ Rinv, -Rinv.T], [-Rinv, np.zeros_like(R)]])
+    W = np.concatenate([S, gamma * Y], axis=1)
+    q = gamma * g + W @ (M @ (W.T @ g))
+    return Control(a0=torch.from_numpy(q.reshape(grd['a0'].shape).copy()))
+
+
+def test_bfgs_fused_direction_hook():
+    """The optimiser's `lbfgs_direction` hook: a hook that returns the direction (here by the compact representation)
+    gives the iterates of the two-loop recursion; a hook that returns None falls back to the recursion."""
+    runs = {}
+    for name, hook in (('recursion', None), ('compact', _compact_lbfgs)):
+        m = _IllConditioned(hook=hook)
+        bfgs_mod.bfgs(m, verb=False, maxIter=25, epsInit=1.0, Wolfe=True, lineSearch='Weak_Wolfe', memory=5)
+        runs[name] = (np.array(m.history), m)
+    (h_rec, m_rec), (h_cmp, m_cmp) = runs['recursion'], runs['compact']
+    assert m_rec.hook_calls >= 5 and m_cmp.hook_calls == m_rec.hook_calls     # called at every iteration with pairs
+    assert h_rec.shape == h_cmp.shape and h_rec.shape[0] >= 6
+    assert np.max(np.abs(h_rec - h_cmp)) <= 1e-10 * np.max(np.abs(h_rec))
+    assert h_cmp[-1] < 1e-4 * h_cmp[0]
