@@ -92,18 +92,33 @@ def _smoother(sigma):
     return K
 
 
+_MASSES = {}
+
+
+def _smoother_mass(sigma, X0):
+    """K_sigma(X0) 1 (N,3): the normaliser of the smoothed features, which depends on the source alone. Cached for
+    the same source tensor object (the entry keeps a reference to it, so its memory cannot be reused by another
+    array) while its in-place version counter is unchanged: pairs sharing a source compute it once."""
+    e = _MASSES.get((sigma, id(X0)))
+    if e is not None and e[0] is X0 and e[1] == X0._version:
+        return e[2]
+    if len(_MASSES) > 16:
+        _MASSES.clear()
+    m = _smoother(sigma).applyK(X0, torch.ones_like(X0))
+    _MASSES[(sigma, id(X0))] = (X0, X0._version, m)
+    return m
+
+
 def pair_features(X0, faces_t, X1, normals=None):
     """(N, IN_DIM) bf16 feature matrix (rows padded to a multiple of 64 with zeros) for source X0 and target X1."""
     n = X0.shape[0]
     nrm = vertex_normals(X0, faces_t) if normals is None else normals
     d = nearest_displacement(X0, X1)
-    ones = torch.ones_like(X0)
     dn = (d * nrm).sum(dim=1, keepdim=True)
     dl = d.norm(dim=1, keepdim=True)
     feats = [X0 - X0.mean(dim=0, keepdim=True), nrm, d]
     for s in (0.25, 0.5):
-        K = _smoother(s)
-        feats.append(K.applyK(X0, d) / K.applyK(X0, ones))
+        feats.append(_smoother(s).applyK(X0, d) / _smoother_mass(s, X0))
     feats += [dn, dl]
     scal = torch.cat([dn, dl, torch.ones_like(dn)], dim=1).contiguous()   # one kernel sum smooths both and the mass
     for s in SCALAR_WIDTHS:

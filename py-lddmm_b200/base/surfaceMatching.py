@@ -64,7 +64,8 @@ class _DeviceMatching:
                 'affineKernel': False, 'testGradient': False, 'Landmarks': None, 'saveFile': 'evolution',
                 'saveRate': 10, 'mode': 'normal', 'verb': True, 'pplot': False, 'outputDir': '.',
                 'symmetric': False, 'internalCost': None, 'lineSearch': 'Weak_Wolfe', 'gradTol': -1.,
-                'gradLB': 0.001, 'initialMomentum': None, 'targetObjective': None, 'processGroup': None}
+                'gradLB': 0.001, 'initialMomentum': None, 'targetObjective': None, 'processGroup': None,
+                'warmStart': None}
 
     def __init__(self, Template=None, Target=None, options=None):
         self.options = self.getDefaultOptions()
@@ -309,6 +310,20 @@ class _DeviceMatching:
         return path
 
     def optimizeMatching(self):
+        ws = self.options.get('warmStart')
+        if ws is not None and not getattr(self, '_warm_started', False):
+            # learned / coarse-to-fine warm start (SecondOrderSurfaceMatching): {'model': MomentumProposal or None,
+            # 'coarse': [(faces, vertices), ...] coarsest first, optional 'rtol'}; the record is kept in
+            # self.warmStartRecord
+            if self.control_key != 'a0':
+                raise NotImplementedError('options["warmStart"] applies to SecondOrderSurfaceMatching')
+            from .learnedProposal import multilevel_warm_start, warm_start
+            if ws.get('coarse'):
+                self.warmStartRecord = multilevel_warm_start(self, ws.get('model'), ws['coarse'],
+                                                             rtol=ws.get('rtol', 1e-4))
+            elif ws.get('model') is not None:
+                self.warmStartRecord = warm_start(self, ws['model'], scales=ws.get('scales', (0.5, 0.75, 1.0)))
+            self._warm_started = True
         grd = self.getGradient(self.gradCoeff)
         [grd2] = self.dotProduct_euclidean(grd, [grd])
         if self.gradEps < 0:

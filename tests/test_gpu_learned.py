@@ -205,6 +205,16 @@ def test_multilevel_warm_start_reaches_the_plain_optimum_sooner():
     it_plain = next(k for k, v in enumerate(plain.history) if v <= target * (1 + 1e-9))
     it_warm = next((k for k, v in enumerate(warm.history) if v <= target * (1 + 1e-9)), len(warm.history))
     assert it_warm < it_plain, (it_warm, it_plain)
+    # the same warm start through the options of the matching class: the same start and the same iterates
+    via = matching()
+    via.options['warmStart'] = {'model': model, 'coarse': [icosphere(2)[::-1], icosphere(3)[::-1]], 'rtol': 1e-4}
+    via.optimizeMatching()
+    got, want = via.warmStartRecord['levels'], rec['levels']
+    assert [lv['iters'] for lv in got] == [lv['iters'] for lv in want]
+    # the vertex normals of the features are summed with atomic adds: agreement to rounding, not bitwise
+    assert np.allclose([lv['objective'] for lv in got], [lv['objective'] for lv in want], rtol=1e-9, atol=0)
+    assert len(via.history) == len(warm.history)
+    assert np.allclose(via.history, warm.history, rtol=1e-6, atol=0)
 
 
 def test_shapes_law_pairs():
