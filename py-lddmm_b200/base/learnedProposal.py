@@ -271,7 +271,7 @@ def _shape_field(X0, gen, rng, Ksm):
 
 
 def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, timeStep=0.1, vmin=0.05, vmax=0.35,
-                   law='noise'):
+                   law='noise', graph=True):
     """Features (n_pairs, Mpad, IN_DIM) bf16, labels (n_pairs, Mpad, 3) f32 and momenta (n_pairs, n, 3) f64 of pairs
     (x0, shoot(x0, a_i)).
 
@@ -279,7 +279,12 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     (several widths: a sum of such fields, one per width, with random weights U[0, 1]);
     targets shot with K_{sigma_def} over round(1/timeStep) steps; labels are the momentum densities a_i * mass
     (mass of K_{sigma_def}), over MOMENTUM_SCALE. law='shapes' draws the scalar field from the law of
-    MOMENTUM_LAW_SHAPES instead of smoothed noise alone."""
+    MOMENTUM_LAW_SHAPES instead of smoothed noise alone.
+
+    With `graph` the part of a pair after its random field -- the speed rescale, the shooting, the features and the
+    label, ~30 launches of small level-4 kernels -- is captured once in a CUDA graph and replayed per pair (static
+    input and output buffers), so the host issues one replay instead of the launches; the results are those of the
+    eager path."""
     X0 = nat.as_device(x0)
     faces_t = torch.from_numpy(np.ascontiguousarray(faces, dtype=np.int64)).cuda()
     n = X0.shape[0]
@@ -303,7 +308,8 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
     if law not in ('noise', 'shapes'):
         raise ValueError(f'unknown momentum law {law!r}')
     rng = np.random.default_rng(seed)
-    for i in range(n_pairs):
+
+    def field():
         a = torch.zeros_like(X0)
         if law == 'shapes':
             a = _shape_field(X0, gen, rng, Ksm[0]) * normals
@@ -312,11 +318,41 @@ def generate_pairs(x0, faces, n_pairs, seed=0, sigma_def=0.5, sigma_smooth=0.4, 
             f = k.applyK(X0, z)[:, :1]
             wt = torch.rand((), generator=gen, dtype=torch.float64, device='cuda') if len(Ksm) > 1 else 1.0
             a = a + wt * f / f.abs().max() * normals
-        v = Kdef.applyK(X0, a)
-        a = a * (speeds[i] / v.norm(dim=1).max())
+        return a
+
+    def finish(a_raw, speed):
+        v = Kdef.applyK(X0, a_raw)
+        a = a_raw * (speed / v.norm(dim=1).max())
         xt, _ = evol.shoot_second_order(X0, a, Kdef, timeStep, origin=origin)
-        feats[i] = pair_features(X0, faces_t, xt[-1], normals)
-        labels[i, :n] = (a * mass / MOMENTUM_SCALE).to(torch.float32)
+        return a, pair_features(X0, faces_t, xt[-1], normals), (a * mass / MOMENTUM_SCALE).to(torch.float32)
+
+    if graph and n_pairs > 1:
+        a_in = torch.zeros_like(X0)
+        s_in = torch.zeros((), dtype=torch.float64, device='cuda')
+        a_in.copy_(normals)
+        s_in.fill_(0.5 * (vmin + vmax))
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):      # warm-up: workspaces and cached normalisers exist before the capture
+            for _ in range(2):
+                finish(a_in, s_in)
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            a_out, f_out, l_out = finish(a_in, s_in)
+        for i in range(n_pairs):
+            a_in.copy_(field())
+            s_in.copy_(speeds[i])
+            g.replay()
+            feats[i] = f_out
+            labels[i, :n] = l_out
+            momenta[i] = a_out
+        del g
+        return feats, labels, momenta, n
+    for i in range(n_pairs):
+        a, f, lab = finish(field(), speeds[i])
+        feats[i] = f
+        labels[i, :n] = lab
         momenta[i] = a
     return feats, labels, momenta, n
 

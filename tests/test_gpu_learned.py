@@ -242,3 +242,16 @@ def test_shapes_law_pairs():
     # the vertex normals are accumulated with atomic adds (index_add_), so a second draw agrees to rounding
     _, _, again, _ = lp.generate_pairs(x0, F, 8, seed=5, timeStep=0.1, law='shapes', vmin=0.1, vmax=0.3)
     assert rel_err(again.cpu().numpy(), momenta.cpu().numpy()) < 1e-12
+
+
+def test_generate_pairs_graph_replay_matches_eager():
+    """The CUDA-graph replay of a pair's pipeline (speed rescale, shooting, features, label) gives the eager path's
+    features, labels and momenta (to the rounding of the atomically summed vertex normals)."""
+    from base import learnedProposal as lp
+    from base.syntheticShapes import icosphere
+    x0, F = icosphere(3)
+    out = {g: lp.generate_pairs(x0, F, 6, seed=9, timeStep=0.1, law='shapes', graph=g) for g in (True, False)}
+    (fg, lg, mg, _), (fe, le, me, _) = out[True], out[False]
+    assert rel_err(mg.cpu().numpy(), me.cpu().numpy()) < 1e-12
+    assert rel_err(lg.double().cpu().numpy(), le.double().cpu().numpy()) < 1e-6
+    assert rel_err(fg.float().cpu().numpy(), fe.float().cpu().numpy()) < 1e-2     # bf16 features
