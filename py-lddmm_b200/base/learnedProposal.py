@@ -486,7 +486,7 @@ def multilevel_warm_start(matching, model, coarse_templates, rtol=1e-4, window=3
     for faces, verts in coarse_templates:
         opts = dict(o)
         opts.update(KparDiff=deepcopy(o['KparDiff']), KparDist=deepcopy(o['KparDist']), maxIter=max_iter,
-                    targetObjective=None, verb=False, processGroup=None,
+                    targetObjective=None, verb=False, processGroup=None, warmStart=None,
                     initialMomentum=None if a_prev is None else prolong_momentum(x_prev, a_prev, verts,
                                                                                   o['KparDiff'], h_prev))
         level = SecondOrderSurfaceMatching(Template=(faces, verts), Target=target, options=opts)
