@@ -34,6 +34,8 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
     dot_dev = getattr(opt, 'dotProduct_device', None)
     # optional: (gradient, history) -> the two-loop recursion's direction in one call, or None to run it here
     fused_direction = getattr(opt, 'lbfgs_direction', None)
+    # optional: (objective, |gradient|^2) -> the first step along the gradient, or None for 1 / |gradient|
+    initial_step = getattr(opt, 'initial_step', None)
     addProd = getattr(opt, 'addProd', lambda x, y, a: x + a * y)
     prod = getattr(opt, 'prod', lambda x, a: a * x)
     copyDir = getattr(opt, 'copyDir', deepcopy)
@@ -129,6 +131,10 @@ def bfgs(opt, verb=True, maxIter=1000, TestGradient=False, epsInit=0.01, memory=
         grdTry = np.sqrt(np.maximum(1e-20, dot(q, [q])[0]))
         dir0 = copyDir(q)
         t_init = 1. / grdTry if (it == 0 or opt.reset) else 1.
+        if it == 0 and not opt.reset and initial_step is not None:
+            t_hint = initial_step(obj, grd2)
+            if t_hint is not None:
+                t_init = t_hint
         grdOld = copyDir(grd)
 
         if it == 0 or it == burnIn:

@@ -462,7 +462,7 @@ def _refine(matching, rtol, window):
 
 
 def multilevel_warm_start(matching, model, coarse_templates, rtol=1e-4, window=3, max_iter=200, width_factor=0.4,
-                          scales=(0.5, 0.75, 1.0)):
+                          scales=(0.5, 0.75, 1.0), first_step_gap=1e-3):
     """The learned warm start refined coarse to fine, for a SecondOrderSurfaceMatching `matching` (not yet
     optimised).
 
@@ -473,7 +473,9 @@ def multilevel_warm_start(matching, model, coarse_templates, rtol=1e-4, window=3
     iterations (or `max_iter`), and `prolong_momentum` carries it to the next level (interpolation width
     `width_factor` x the coarse mean edge length). At the level of `matching` the prolonged momentum is the
     proposal: it becomes the control when it lowers the objective (the plain optimiser's zero start is the fallback),
-    and `matching.optimizeMatching()` then refines from there.
+    and `matching.optimizeMatching()` then refines from there, its first step along the gradient sized for a
+    decrease of `first_step_gap` x the objective (`initial_step` of the matching; None: the optimiser's unit step,
+    which at this distance from the optimum overshoots ~10^4-fold and costs ~5 extra objective evaluations).
 
     Returns a record: per level its vertex count, iterations and objective, whether the network's proposal was
     taken, and whether the fine level took the prolonged momentum."""
@@ -508,5 +510,7 @@ def multilevel_warm_start(matching, model, coarse_templates, rtol=1e-4, window=3
     used = bool(np.isfinite(o_try) and o_try < obj_here)
     if used:
         matching.acceptVarTry()
-    rec.update(prolonged_used=used, obj_prolonged=float(o_try), obj_start=float(obj_here))
+        matching.first_step_gap = first_step_gap
+    rec.update(prolonged_used=used, obj_prolonged=float(o_try), obj_start=float(obj_here),
+               first_step_gap=first_step_gap if used else None)
     return rec

@@ -221,6 +221,22 @@ class _DeviceMatching:
     # spread over the GPU.
     LBFGS_FUSED_MAX = 1 << 16
 
+    # Expected decrease of the objective along the first gradient step, as a fraction of the objective, set by a
+    # warm start (None: the optimiser's own first step, 1 / |gradient|, as in the reference).
+    first_step_gap = None
+
+    def initial_step(self, obj, grd2):
+        """The optimiser's first step along -gradient after a warm start: the minimiser t = 2 D / |g|^2 of the
+        quadratic model phi(t) = f0 - |g|^2 t + h t^2 / 2 whose minimum lies D = first_step_gap * f0 below f0
+        (the initial-step rule 2 (f_k - f_k-1) / phi'(0) of Nocedal & Wright, section 3.5, with the expected
+        decrease in place of the previous one). Near an optimum a unit step (1 / |g|) overshoots by orders of
+        magnitude and the line search shrinks it one objective evaluation at a time; any D within 10x of the
+        true decrease passes in one or two. Used once; None leaves the optimiser's rule."""
+        gap, self.first_step_gap = self.first_step_gap, None
+        if gap is None or not (grd2 > 0) or not np.isfinite(obj) or obj <= 0:
+            return None
+        return 2.0 * gap * obj / (self.gradCoeff * grd2)
+
     def lbfgs_direction(self, grd, history):
         """The optimiser's two-loop recursion (base/bfgs.py:183-198) for gradient `grd` and the stored pairs
         `history` ([s_k, y_k], oldest first) in one call of lddmm_lbfgs_direction, or None when the controls do not
@@ -313,14 +329,15 @@ class _DeviceMatching:
         ws = self.options.get('warmStart')
         if ws is not None and not getattr(self, '_warm_started', False):
             # learned / coarse-to-fine warm start (SecondOrderSurfaceMatching): {'model': MomentumProposal or None,
-            # 'coarse': [(faces, vertices), ...] coarsest first, optional 'rtol'}; the record is kept in
-            # self.warmStartRecord
+            # 'coarse': [(faces, vertices), ...] coarsest first, optional 'rtol' and 'first_step_gap'}; the record
+            # is kept in self.warmStartRecord
             if self.control_key != 'a0':
                 raise NotImplementedError('options["warmStart"] applies to SecondOrderSurfaceMatching')
             from .learnedProposal import multilevel_warm_start, warm_start
             if ws.get('coarse'):
                 self.warmStartRecord = multilevel_warm_start(self, ws.get('model'), ws['coarse'],
-                                                             rtol=ws.get('rtol', 1e-4))
+                                                             rtol=ws.get('rtol', 1e-4),
+                                                             first_step_gap=ws.get('first_step_gap', 1e-3))
             elif ws.get('model') is not None:
                 self.warmStartRecord = warm_start(self, ws['model'], scales=ws.get('scales', (0.5, 0.75, 1.0)))
             self._warm_started = True

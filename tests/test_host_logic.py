@@ -190,3 +190,35 @@ def test_bfgs_fused_direction_hook():
     assert h_rec.shape == h_cmp.shape and h_rec.shape[0] >= 6
     assert np.max(np.abs(h_rec - h_cmp)) <= 1e-10 * np.max(np.abs(h_rec))
     assert h_cmp[-1] < 1e-4 * h_cmp[0]
+
+
+def test_bfgs_initial_step_hook():
+    """The first step after a warm start (`first_step_gap`): started near the optimum of the ill-conditioned
+    quadratic, the optimiser's own first trial (1 / |g|) overshoots and the line search shrinks it over several
+    objective evaluations; with the expected decrease given, the first trial is 2 D / |g|^2 and is accepted at once.
+    Without the gap the hook leaves the optimiser's rule (the reference's first step)."""
+    trials = {}
+    for gap in (None, 'exact'):
+        m = _IllConditioned()
+        m.control = Control(a0=m.c + 1e-3 * torch.cos(torch.arange(3 * m.npt, dtype=torch.float64)).reshape(m.npt, 3))
+        m.obj = None
+        f0 = m.objectiveFun()
+        g = m.D * (m.control['a0'] - m.c)
+        g2 = float((g * g).sum())
+        if gap == 'exact':   # the decrease of the exact line minimum along -g: (g.g)^2 / (2 g.D g)
+            m.first_step_gap = g2 ** 2 / (2 * float((g * m.D * g).sum())) / f0
+        seen = []
+        update_try = m.updateTry
+
+        def record(dr, eps, objRef=None, update_try=update_try, seen=seen):
+            seen.append(float(eps))
+            return update_try(dr, eps, objRef)
+        m.updateTry = record
+        bfgs_mod.bfgs(m, verb=False, maxIter=1, epsInit=1.0, Wolfe=True, lineSearch='Weak_Wolfe', memory=5)
+        trials[gap] = (seen, m.obj, f0, g2)
+        assert m.first_step_gap is None                     # used once
+    seen, obj, f0, g2 = trials[None]
+    assert seen[0] == pytest.approx(1 / np.sqrt(g2)) and len(seen) >= 3 and obj < f0
+    seen_h, obj_h, f0_h, _ = trials['exact']
+    assert f0_h == f0 and len(seen_h) == 1 and obj_h < f0
+    assert seen_h[0] < seen[0] / 10
