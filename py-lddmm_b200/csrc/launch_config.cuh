@@ -1,6 +1,7 @@
 // Launch shapes of the all-pairs kernels (threads per CTA x targets per thread). The defaults were chosen by
 // timing on the B200; each can be overridden at build time (-DLDDMM_RT_LIGHT=... etc.) for tuning sweeps.
 #pragma once
+#include <stdint.h>
 
 #ifndef LDDMM_TPB_LIGHT
 #define LDDMM_TPB_LIGHT 128
@@ -22,6 +23,15 @@
 #endif
 #ifndef LDDMM_RT_FO_SYM
 #define LDDMM_RT_FO_SYM 4
+#endif
+#ifndef LDDMM_RT_SYM_SMALL
+#define LDDMM_RT_SYM_SMALL 2
+#endif
+#ifndef LDDMM_SYM_FWD_SMALL_N
+#define LDDMM_SYM_FWD_SMALL_N 16384
+#endif
+#ifndef LDDMM_SYM_ADJ_SMALL_N
+#define LDDMM_SYM_ADJ_SMALL_N 6144
 #endif
 #ifndef LDDMM_RT_SYM_FWD_L
 #define LDDMM_RT_SYM_FWD_L 4
@@ -65,6 +75,14 @@ constexpr int kRtAdjoint = LDDMM_RT_ADJOINT;
 // thread (134 registers, 3 CTAs per SM): the per-step source loads and the column shuffles are shared by twice
 // as many pairs, and four independent lane groups hide the latency of the ex2 chain.
 constexpr int kRtSymFwd = LDDMM_RT_SYM_FWD;
+// Small point sets (the coarse levels of a coarse-to-fine registration): row blocks of 256 points instead of 1,024
+// (forward) or 512 (adjoint), so that the unit triangle gives the GPU ~10x more units. At level 4 (2,562 points)
+// 1,024-point blocks leave 39 units for 444 resident CTAs and a step is latency-bound (39.5 us forward, 39.4 us
+// adjoint, with the epilogue); 2 targets per thread: 27.2 and 31.2 us. At level 5 (10,242) the forward step
+// still gains (123.5 -> 95.7 us) and the adjoint step loses (134.4 -> 146.6 us); at level 6 both lose 30-40%.
+constexpr int kRtSymSmall = LDDMM_RT_SYM_SMALL;
+constexpr int64_t kSymFwdSmallN = LDDMM_SYM_FWD_SMALL_N;  // Gaussian forward step: 2 targets per thread up to here
+constexpr int64_t kSymAdjSmallN = LDDMM_SYM_ADJ_SMALL_N;  // Gaussian adjoint step: 2 targets per thread up to here
 // The symmetric K(x, x) a (pairs_kernel_symx): 8 targets per thread.
 // The symmetric first-order adjoint step (pairs_kernel_sym): 4 targets per thread.
 constexpr int kRtFoSym = LDDMM_RT_FO_SYM;

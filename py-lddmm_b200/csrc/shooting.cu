@@ -460,6 +460,8 @@ size_t shooting_ws_bytes(int64_t n, int precision) {
     if (LDDMM_SYM) {
       upd(sym_ws_bytes<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(n));
       upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymFwd>(n));
+      if (n <= kSymAdjSmallN) upd(sym_ws_bytes<OpSOBwdSym, kTpbHeavy, kRtSymSmall>(n));
+      if (n <= kSymFwdSmallN) upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymSmall>(n));
       upd(sym_ws_bytes<OpFOBwdSym, kTpbLight, kRtFoSym>(n));
       upd(sym_ws_bytes<OpSOBwdSym, kTpbHeavy, kRtAdjointSymL, Laplacian>(n));
       upd(sym_ws_bytes<OpSOFwdSym, kTpbLight, kRtSymFwdL, Laplacian>(n));
@@ -548,6 +550,8 @@ int so_step(const double* x, const double* a, int64_t n, const Frame& f, double 
   const int64_t rows = nrows < 0 ? n : nrows;
   if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
     if (row0 == 0 && rows == n) {
+      if (f.family == kGauss && n <= kSymFwdSmallN)
+        return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymSmall>(P, n, ws, wsb, st);
       if (f.family == kGauss) return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymFwd>(P, n, ws, wsb, st);
       return run_pairs_sym<OpSOFwdSym, kTpbLight, kRtSymFwdL, Laplacian>(P, n, ws, wsb, st);
     }
@@ -563,6 +567,8 @@ int so_adjoint_step(const double* x, const double* a, const double* px, const do
   const int64_t rows = nrows < 0 ? n : nrows;
   if constexpr (std::is_same<V, F2>::value && LDDMM_SYM != 0) {
     if (row0 == 0 && rows == n) {
+      if (f.family == kGauss && n <= kSymAdjSmallN)
+        return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtSymSmall>(P, n, ws, wsb, st);
       if (f.family == kGauss) return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtAdjoint>(P, n, ws, wsb, st);
       return run_pairs_sym<OpSOBwdSym, kTpbHeavy, kRtAdjointSymL, Laplacian>(P, n, ws, wsb, st);
     }
