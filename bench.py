@@ -405,8 +405,10 @@ def _register(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=None, model
     (coarser triangulations (faces, vertices) of the source, coarsest first) the warm start is the coarse-to-fine one
     (learnedProposal.multilevel_warm_start, with the network at the coarsest level when `model` is given);
     otherwise the network's proposal at this level (learnedProposal.warm_start) when `model` is given."""
+    import gc
     import torch
     from base import learnedProposal as lp
+    gc.collect()            # not inside the timed region: a cyclic-GC pass there would land on one run at random
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     f = _matching(x0, F, x1, dtype, sigma, sigma_dist, time_step, target=target, maxIter=maxIter, a0=a0)
@@ -425,13 +427,12 @@ WARM_REPEATS = 3
 
 
 def _register_median(*a, repeats=WARM_REPEATS, **k):
-    """_register `repeats` times: (matching and record of the median run, median seconds, every sample)."""
-    import torch
+    """_register `repeats` times: (matching and record of the median run, median seconds, every sample). The caching
+    allocator keeps its blocks between the repeats (no cudaMalloc inside the timed region after the first)."""
     runs = []
     for _ in range(repeats):
         f, _, t, used = _register(*a, **k)
         runs.append((t, f, used))
-        torch.cuda.empty_cache()
     runs.sort(key=lambda r: r[0])
     t, f, used = runs[len(runs) // 2]
     return f, t, [r[0] for r in runs], used
@@ -593,7 +594,6 @@ def run_registration(args):
             ('learned_multilevel_fp32', model, coarse))
     # untimed: the first run of the coarse-to-fine path (its level-4 plans and workspaces, the prolongation's masses)
     _register(x0, F, x1, 'float32', sig, sigd, ts, target=target, model=model, coarse=coarse)
-    torch.cuda.empty_cache()
     for name, model_, coarse_ in runs:
         if coarse_ is None:
             f, t0, t, used = _register(x0, F, x1, 'float32', sig, sigd, ts, target=target, model=model_)
@@ -615,7 +615,6 @@ def run_registration(args):
             res[name].update({'proposal_used': used[0], 'obj_proposal': used[1], 'obj_zero': used[2],
                               'scale': used[3]})
         del f
-        torch.cuda.empty_cache()
     p64 = res['plain_fp64']['s_per_pair']
     res['speedup_learned_vs_plain_fp64'] = p64 / res['learned_multilevel_fp32']['s_per_pair']
     res['speedup_learned_single_level_vs_plain_fp64'] = p64 / res['learned_fp32']['s_per_pair']
