@@ -291,29 +291,64 @@ __global__ void __launch_bounds__(TPB, Op::kSymMinCtas)
   }
 }
 
-// Epilogue: row slots of the point's block (in CTA order), then its column partials (in block order), in FP64.
+// Epilogue: the row slots of the point's block and its column partials, in FP64, summed by TPP threads per point
+// (TPP a power of two <= 32). A CTA of kFinThreads threads takes P = kFinThreads / TPP consecutive points; thread
+// (j, p) -- p = threadIdx % P, j = threadIdx / P -- sums slots j, j + TPP, ... and column partials j, j + TPP, ...
+// of point p (consecutive threads read consecutive points: coalesced), and thread (0, p) adds the TPP sums in the
+// order j = 0, 1, ... from shared memory and applies the op's epilogue. Every addition's order is fixed by (point,
+// TPP): deterministic. With one thread per point, a point's slots and partials are one serial chain of up to tens
+// of dependent loads (at 2,562 points: 11 CTAs, ~11 us, latency-bound); several threads shorten the chain and
+// spread the points over more CTAs.
+constexpr int kFinThreads = 256;
 template <class Op, int TPB, int RT>
-__global__ void finalize_sym_kernel(const typename Op::Params P, int n, int nblk, int TT, long long U, int C,
-                                    const float2* __restrict__ row_ws, const float* __restrict__ col_ws) {
-  constexpr int B = TPB * RT;
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  double row[Op::NR], col[Op::NC];
+__global__ void __launch_bounds__(kFinThreads)
+    finalize_sym_kernel(const typename Op::Params P, int n, int nblk, int TT, long long U, int C,
+                        const float2* __restrict__ row_ws, const float* __restrict__ col_ws, int tpp) {
+  constexpr int B = TPB * RT, NV = Op::NR + Op::NC;
+  __shared__ double red[kFinThreads][NV];
+  const int np = kFinThreads / tpp;
+  const int p = threadIdx.x % np, j = threadIdx.x / np;
+  const int idx = blockIdx.x * np + p;
+  const bool live = idx < n;
+  double v[NV];
 #pragma unroll
-  for (int c = 0; c < Op::NR; ++c) row[c] = 0.0;
+  for (int c = 0; c < NV; ++c) v[c] = 0.0;
+  const int b = live ? idx / B : 0, r = live ? idx - b * B : 0;
+  if (live) {
+    const int nslot = sk_cta_of(sym_row_off(b + 1, TT, RT) - 1, U, C) - sk_cta_of(sym_row_off(b, TT, RT), U, C) + 1;
+    for (int s = j; s < nslot; s += tpp)
 #pragma unroll
-  for (int c = 0; c < Op::NC; ++c) col[c] = 0.0;
-  const int b = idx / B, r = idx - b * B;
-  const int nslot = sk_cta_of(sym_row_off(b + 1, TT, RT) - 1, U, C) - sk_cta_of(sym_row_off(b, TT, RT), U, C) + 1;
-  for (int s = 0; s < nslot; ++s)
+      for (int c = 0; c < Op::NR; ++c) v[c] += partial_value(row_ws[((size_t)s * Op::NR + c) * (size_t)n + idx]);
+    for (int q = j; q < b; q += tpp) {
+      const size_t cb = (size_t)(sym_tri(b) + q) * Op::NC * B + r;
 #pragma unroll
-    for (int c = 0; c < Op::NR; ++c) row[c] += partial_value(row_ws[((size_t)s * Op::NR + c) * (size_t)n + idx]);
-  for (int q = 0; q < b; ++q) {
-    const size_t cb = (size_t)(sym_tri(b) + q) * Op::NC * B + r;
-#pragma unroll
-    for (int c = 0; c < Op::NC; ++c) col[c] += (double)col_ws[cb + (size_t)c * B];
+      for (int c = 0; c < Op::NC; ++c) v[Op::NR + c] += (double)col_ws[cb + (size_t)c * B];
+    }
   }
-  Op::finalize_sym(P, idx, row, col);
+  if (tpp > 1) {
+#pragma unroll
+    for (int c = 0; c < NV; ++c) red[threadIdx.x][c] = v[c];
+    __syncthreads();
+    if (j == 0)
+      for (int k = 1; k < tpp; ++k)
+#pragma unroll
+        for (int c = 0; c < NV; ++c) v[c] += red[k * np + p][c];
+  }
+  if (live && j == 0) Op::finalize_sym(P, idx, v, v + Op::NR);
+}
+
+// Threads per point of finalize_sym_kernel: enough to split the longest chain of slots and column partials (a row
+// block's slots plus the blocks below it) into pieces of about four, at most 8.
+inline int sym_finalize_tpp(const SymPlan& p) {
+  const int chain = p.S + p.nblk;
+  int t = 1;
+  while (t < 8 && chain > 4 * t) t <<= 1;
+  return t;
+}
+
+inline int sym_finalize_grid(int64_t n, int tpp, int threads) {
+  const int64_t np = threads / tpp;
+  return (int)((n + np - 1) / np);
 }
 
 // Dynamic shared memory of pairs_kernel_sym (its compensated row sums).
@@ -372,9 +407,10 @@ inline int run_pairs_sym(const typename Op::Params& P, int64_t n, void* ws, size
   auto* col_ws = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.col_off);
   pairs_kernel_sym<Op, TPB, RT, Fam><<<plan.C, TPB, sym_dyn_smem_bytes<Op, TPB, RT>(), stream>>>(
       P, (int)n, plan.nblk, plan.TT, plan.U, plan.C, row_ws, col_ws);
-  const int fb = 256;
-  finalize_sym_kernel<Op, TPB, RT><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT, plan.U,
-                                                                                 plan.C, row_ws, col_ws);
+  const int fb = kFinThreads, tpp = sym_finalize_tpp(plan);
+  finalize_sym_kernel<Op, TPB, RT><<<sym_finalize_grid(n, tpp, fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT,
+                                                                                      plan.U, plan.C, row_ws, col_ws,
+                                                                                      tpp);
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
@@ -686,9 +722,10 @@ inline int run_pairs_symx(const typename Op::Params& P, int64_t n, void* ws, siz
   auto* col_ws = reinterpret_cast<float*>(reinterpret_cast<char*>(ws) + plan.col_off);
   pairs_kernel_symx<Op, TPB, RT><<<plan.C, TPB, symx_dyn_smem_bytes<Op, TPB, RT>(), stream>>>(
       P, (int)n, plan.nblk, plan.TT, plan.U, plan.C, row_ws, col_ws);
-  const int fb = 256;
-  finalize_sym_kernel<Op, TPB, RT><<<(int)((n + fb - 1) / fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT, plan.U,
-                                                                                 plan.C, row_ws, col_ws);
+  const int fb = kFinThreads, tpp = sym_finalize_tpp(plan);
+  finalize_sym_kernel<Op, TPB, RT><<<sym_finalize_grid(n, tpp, fb), fb, 0, stream>>>(P, (int)n, plan.nblk, plan.TT,
+                                                                                      plan.U, plan.C, row_ws, col_ws,
+                                                                                      tpp);
   return cudaPeekAtLastError() == cudaSuccess ? kOk : kLaunchFailure;
 }
 
