@@ -77,12 +77,43 @@ def emulate(n, TPB, RT, wave, rng):
             row_ws[slot, rows] = acc
             u += t1 - t0
             i += 1
+    # the epilogue (finalize_sym_kernel): tpp threads per point; thread (j, p) of a CTA of 256 threads sums slots
+    # j, j + tpp, ... and column partials j, j + tpp, ... of point blockIdx * (256 / tpp) + p; thread (0, p) adds the
+    # tpp sums in the order j = 0, 1, ...
+    tpp = finalize_tpp(S, nblk)
+    npc = 256 // tpp
     out = np.zeros(n)
-    for idx in range(n):
-        b, r = idx // B, idx % B
-        nslot = (sk_cta_of(row_off(b + 1, TT, RT) - 1, U, C) - sk_cta_of(row_off(b, TT, RT), U, C) + 1)
-        out[idx] = row_ws[:nslot, idx].sum() + sum(col_ws[(tri(b) + q) * B + r] for q in range(b))
+    for cta in range(-(-n // npc)):
+        for p in range(npc):
+            idx = cta * npc + p
+            if idx >= n:
+                continue
+            b, r = idx // B, idx % B
+            nslot = (sk_cta_of(row_off(b + 1, TT, RT) - 1, U, C) - sk_cta_of(row_off(b, TT, RT), U, C) + 1)
+            assert nslot <= S
+            read_s, read_q, part = [], [], []
+            for j in range(tpp):
+                acc = 0.0
+                for sl in range(j, nslot, tpp):
+                    acc += row_ws[sl, idx]
+                    read_s.append(sl)
+                for q in range(j, b, tpp):
+                    k = (tri(b) + q) * B + r
+                    assert 0 <= k < col_ws.size
+                    acc += col_ws[k]
+                    read_q.append(q)
+                part.append(acc)
+            assert sorted(read_s) == list(range(nslot)) and sorted(read_q) == list(range(b))
+            out[idx] = sum(part)
     return out, Kf @ v, credited
+
+
+def finalize_tpp(S, nblk):
+    """sym_finalize_tpp: threads per point of the epilogue (chains of about four, at most 8)."""
+    t = 1
+    while t < 8 and S + nblk > 4 * t:
+        t *= 2
+    return t
 
 
 @pytest.mark.parametrize('n,TPB,RT,wave', [(1, 128, 4, 296), (100, 128, 4, 296), (511, 32, 4, 7), (513, 32, 4, 7),
